@@ -1,0 +1,1363 @@
+// engine.cu -- the device engine of libexcent_b200: per-vertex state in HBM,
+// the demand-snapshot kernel, the on-device fetch plan for cached chunks, the
+// degree-dispatched push kernels, the hot (degree) cache kernels, staging
+// slots, and the C entry points of include/excent_b200.h that drive them.
+//
+// Reference seams replaced (SPADE-IITJ/ExCent, paths relative to the project):
+//   k_init                         src/excent.cu:41-47
+//   k_snapshot (+ k_compact)       src/excent.cu:49-98, 150-164
+//   push_vertex_g / k_push_*       src/excent.cu:100-148, 166-176, 199-209
+//   k_compact_hot / k_fill_hot     src/excent.cu:178-182, 211-220
+//   launch policy                  src/excent.cu:235-240, 629-652
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "common.h"
+#include "device.cuh"
+
+namespace excent {
+
+static constexpr int SNAP_GROUP = 16;     // bitmap words per warp step in the snapshot (512 vertices)
+static constexpr unsigned SMALL_MAX = 32; // degree <= 32: edge-balanced across the warp
+static constexpr unsigned HUB_MIN = 2048; // degree > 2048: split into segments for whole warps
+static constexpr unsigned HUB_SEG = 2048; // edges per hub segment
+static constexpr int BLOCK = 256;
+
+enum { SRC_TABLE = 0, SRC_CHUNK = 1, SRC_GATHER = 2, SRC_HOT = 3 };
+enum { WT_NONE = 0, WT_LIST = 1, WT_RANGE = 2 };
+
+struct HubSeg {
+    const int* nb;
+    unsigned len;
+    unsigned pad;
+    float4 p;
+};
+
+// Device control block: counters that live across kernels of one pass.
+struct Ctrl {
+    ull hotpend;
+    ull pushed;        // adjacency entries pushed since init
+    ull hub_unused;
+    ull items;         // work items of the cached push in this pass
+    int pass;          // passes that pushed so far
+    int done;          // 1 once a snapshot found nothing pending (or max passes)
+    int err;           // nonzero: a device-side capacity check failed
+    int pad;
+    double rsum[MAXM]; // FP64 sum |r| of the last snapshot
+    unsigned hcount;   // hot pending list length
+    unsigned pad2;
+};
+
+struct PassRec {
+    ull pending, demand, hot_pending, pushed_before;
+    double rsum[MAXM];
+    int n_list, n_range;
+};
+
+struct SnapArgs {
+    int n, nc, words, groups_per_warp;
+    const void* r;
+    DevMeasures M;
+    const ull* idx;
+    const int* cv0;
+    const uint32_t* hot;
+    uint32_t* bitmap;
+    ull* cnt;
+    int* list;
+    uint16_t* trace;
+    Ctrl* ctrl;
+};
+
+struct PushArgs {
+    void* x;
+    void* r;
+    DevMeasures M;
+    const ull* idx;
+    const uint32_t* hot;      // range items skip these (cached high-degree vertices)
+    // SRC_TABLE: chunks from the HBM edge cache per the work table
+    int nc;
+    const int* cv0;
+    const uint8_t* wt_type;
+    const unsigned* wt_prefix; // nc + 1 item prefix
+    const int* list;
+    const int* cache;
+    // SRC_CHUNK: one chunk, list or range, edges at ebase + (idx[v] - e0)
+    int ctype, cv_0;
+    unsigned ccount;
+    const int* ebase;
+    ull e0;
+    // SRC_GATHER: k ids, offsets and edges staged together
+    const int* vids;
+    const ull* off;
+    const int* gedges;
+    unsigned gk;
+    // SRC_HOT: compacted indices into the hot cache
+    const int* hlist;
+    const int* hids;
+    const ull* hoff;
+    const int* hedges;
+    // outputs
+    HubSeg* hubq;
+    ull hub_cap;
+    ull* hub_cnt;
+    Ctrl* ctrl;
+};
+
+// ------------------------------------------------------------------ kernels
+
+template <int L>
+__global__ void k_init(int n, const ull* idx, typename Lane<L>::T* x, typename Lane<L>::T* r, int nm, int k0, int k1,
+                       int k2, float beta, float lambda) {
+    const int kind[3] = {k0, k1, k2};
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n;
+         v += (long long)gridDim.x * blockDim.x) {
+        float xs[3], rs[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            xs[k] = 0.f; rs[k] = 0.f;
+            if (k >= nm) continue;
+            // src/excent.cu:43-45
+            if (kind[k] == 0) { xs[k] = 0.f; rs[k] = 1.f - 0.85f; }
+            else if (kind[k] == 1) { xs[k] = 0.f; rs[k] = beta; }
+            else { xs[k] = 1.f; rs[k] = (float)((double)(idx[v + 1] - idx[v]) / lambda - 1.0); }
+        }
+        if constexpr (L == 1) { x[v] = xs[0]; r[v] = rs[0]; }
+        else { x[v] = make_float4(xs[0], xs[1], xs[2], 0.f); r[v] = make_float4(rs[0], rs[1], rs[2], 0.f); }
+    }
+}
+
+__device__ __forceinline__ int chunk_of(long long v, const int* cv0, int nc) {
+    int lo = 0, hi = nc - 1;  // last chunk with cv0[c] <= v
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (cv0[mid] <= v) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Demand snapshot. Each warp owns a contiguous run of 16-word groups; per
+// group it ballots 512 vertices (one bitmap word per 32), writes the words
+// coalesced, and adds the group's pending count and degree sum to its chunk
+// with one atomic pair (per-lane atomics only where a group straddles a chunk
+// boundary). The same atomic returns the offset at which the group's pending
+// ids are appended to the chunk's list region list[cv0[c] ..]. Integer
+// outputs equal src/excent.cu:69-98 exactly; list order is not defined.
+template <int L>
+__global__ void __launch_bounds__(BLOCK) k_snapshot(SnapArgs a) {
+    typedef typename Lane<L>::T T;
+    const T* r = reinterpret_cast<const T*>(a.r);
+    const int lane = threadIdx.x & 31;
+    const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long ngroups = (a.words + SNAP_GROUP - 1) / SNAP_GROUP;
+    long long g0 = gw * a.groups_per_warp, g1 = g0 + a.groups_per_warp;
+    if (g1 > ngroups) g1 = ngroups;
+    double rs0 = 0, rs1 = 0, rs2 = 0;
+    unsigned hp = 0;
+    for (long long g = g0; g < g1; g++) {
+        const long long w0 = g * SNAP_GROUP;
+        const int nw = (int)min((long long)SNAP_GROUP, (long long)a.words - w0);
+        uint32_t myb = 0;
+        ull mydeg = 0;
+#pragma unroll 4
+        for (int j = 0; j < SNAP_GROUP; j++) {
+            if (j >= nw) break;
+            const long long v = (w0 + j) * 32 + lane;
+            bool pend = false;
+            if (v < a.n) {
+                const T rv = r[v];
+                if constexpr (L == 1) rs0 += fabs((double)rv);
+                else {
+                    rs0 += fabs((double)rv.x);
+                    rs1 += fabs((double)rv.y);
+                    rs2 += fabs((double)rv.z);
+                }
+                pend = pending_of(rv, a.M);
+                if (a.trace && pend) a.trace[v]++;
+                if (a.hot && pend && bit_of(a.hot, v)) { hp++; pend = false; }
+                if (pend) mydeg += a.idx[v + 1] - a.idx[v];
+            }
+            const uint32_t b = __ballot_sync(FULL, pend);
+            if (lane == j) myb = b;
+        }
+        if (lane < nw) a.bitmap[w0 + lane] = myb;
+        const unsigned cl = lane < nw ? (unsigned)__popc(myb) : 0u;
+        const unsigned tot = __shfl_sync(FULL, warp_incl_scan(cl, lane), 31);
+        if (tot == 0) continue;
+        const long long vfirst = w0 * 32;
+        long long vlast = (w0 + nw) * 32 - 1;
+        if (vlast >= a.n) vlast = a.n - 1;
+        const int c = chunk_of(vfirst, a.cv0, a.nc);
+        const bool one = (c + 1 >= a.nc) || (vlast < a.cv0[c + 1]);
+        if (one) {
+            const ull dsum = warp_sum(mydeg);
+            unsigned base = 0;
+            if (lane == 0) {
+                base = (unsigned)atomicAdd(&a.cnt[2 * c], (ull)tot);
+                atomicAdd(&a.cnt[2 * c + 1], dsum);
+            }
+            base = __shfl_sync(FULL, base, 0);
+            const unsigned excl = warp_incl_scan(cl, lane) - cl;
+            int* out = a.list + a.cv0[c] + base;
+            for (int j = 0; j < nw; j++) {
+                const uint32_t b = __shfl_sync(FULL, myb, j);
+                const unsigned e = __shfl_sync(FULL, excl, j);
+                if ((b >> lane) & 1u) out[e + __popc(b & ((1u << lane) - 1u))] = (int)((w0 + j) * 32 + lane);
+            }
+        } else {
+            // the group straddles chunk boundaries: group lanes by chunk, per word
+            for (int j = 0; j < nw; j++) {
+                const uint32_t b = __shfl_sync(FULL, myb, j);
+                if (!b) continue;
+                const long long v = (w0 + j) * 32 + lane;
+                const bool pend = (b >> lane) & 1u;
+                const int cc = pend ? chunk_of(v, a.cv0, a.nc) : -1;
+                uint32_t rem = b;
+                while (rem) {
+                    const int leader = __ffs(rem) - 1;
+                    const int cl2 = __shfl_sync(FULL, cc, leader);
+                    const uint32_t mm = __ballot_sync(FULL, pend && cc == cl2);
+                    const ull d = (pend && cc == cl2) ? a.idx[v + 1] - a.idx[v] : 0;
+                    const ull ds = __shfl_sync(FULL, warp_sum(d), 0);
+                    unsigned base = 0;
+                    if (lane == leader) {
+                        base = (unsigned)atomicAdd(&a.cnt[2 * cl2], (ull)__popc(mm));
+                        atomicAdd(&a.cnt[2 * cl2 + 1], ds);
+                    }
+                    base = __shfl_sync(FULL, base, leader);
+                    if ((mm >> lane) & 1u) a.list[a.cv0[cl2] + base + __popc(mm & ((1u << lane) - 1u))] = (int)v;
+                    rem &= ~mm;
+                }
+            }
+        }
+    }
+    // FP64 termination residual and hot pending count: block reduction, one atomic each
+    __shared__ double s_rs[3][BLOCK / 32];
+    __shared__ unsigned s_hp[BLOCK / 32];
+    rs0 = warp_sum(rs0); rs1 = warp_sum(rs1); rs2 = warp_sum(rs2);
+    hp = warp_sum(hp);
+    const int wib = threadIdx.x >> 5;
+    if (lane == 0) { s_rs[0][wib] = rs0; s_rs[1][wib] = rs1; s_rs[2][wib] = rs2; s_hp[wib] = hp; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t0 = 0, t1 = 0, t2 = 0;
+        unsigned th = 0;
+        for (int i = 0; i < BLOCK / 32; i++) { t0 += s_rs[0][i]; t1 += s_rs[1][i]; t2 += s_rs[2][i]; th += s_hp[i]; }
+        atomicAdd(&a.ctrl->rsum[0], t0);
+        if (a.M.nm > 1) atomicAdd(&a.ctrl->rsum[1], t1);
+        if (a.M.nm > 2) atomicAdd(&a.ctrl->rsum[2], t2);
+        if (th) atomicAdd(&a.ctrl->hotpend, (ull)th);
+    }
+}
+
+// On-device fetch plan for a fully cached graph: per chunk with pending
+// vertices choose its pending list (cnt < list_frac * vertices) or its whole
+// range (src/excent.cu:639), build the item prefix, log the pass, decide
+// termination (src/excent.cu:680, max passes :656), reset the counters the
+// next snapshot accumulates into, and set the graph's loop condition.
+__global__ void k_plan(int nc, const int* cv0, int n, ull* cnt, const uint8_t* cmode, double list_frac, int max_passes,
+                       uint8_t* wt_type, unsigned* wt_prefix, Ctrl* ctrl, ull* hub_cnt, PassRec* log, int log_cap,
+                       cudaGraphConditionalHandle cond, int use_cond) {
+    __shared__ ull s_pend, s_dem;
+    __shared__ unsigned s_carry;
+    __shared__ int s_nl, s_nr;
+    __shared__ unsigned s_scan[1024];
+    const int t = threadIdx.x;
+    if (t == 0) { s_pend = 0; s_dem = 0; s_carry = 0; s_nl = 0; s_nr = 0; }
+    __syncthreads();
+    ull lp = 0, ld = 0;
+    for (int c = t; c < nc; c += blockDim.x) { lp += cnt[2 * c]; ld += cnt[2 * c + 1]; }
+    atomicAdd(&s_pend, lp);
+    atomicAdd(&s_dem, ld);
+    __syncthreads();
+    const ull pend = s_pend, dem = s_dem, hp = ctrl->hotpend;
+    const int p = ctrl->pass;
+    const bool stop = ctrl->done || p >= max_passes || (pend == 0 && hp == 0);
+    // work table, scanned in tiles of blockDim.x chunks
+    for (int base = 0; base < nc; base += blockDim.x) {
+        const int c = base + t;
+        unsigned items = 0;
+        uint8_t ty = WT_NONE;
+        if (!stop && c < nc && cmode[c] && cnt[2 * c] > 0) {
+            const int v0 = cv0[c], v1 = c + 1 < nc ? cv0[c + 1] : n;
+            if ((double)cnt[2 * c] < list_frac * (v1 - v0)) { ty = WT_LIST; items = (unsigned)cnt[2 * c]; atomicAdd(&s_nl, 1); }
+            else { ty = WT_RANGE; items = (unsigned)(v1 - v0); atomicAdd(&s_nr, 1); }
+        }
+        s_scan[t] = items;
+        __syncthreads();
+        for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+            unsigned v = t >= o ? s_scan[t - o] : 0;
+            __syncthreads();
+            s_scan[t] += v;
+            __syncthreads();
+        }
+        if (c < nc) { wt_type[c] = ty; wt_prefix[c + 1] = s_carry + s_scan[t]; }
+        if (c == 0) wt_prefix[0] = 0;
+        __syncthreads();
+        if (t == blockDim.x - 1) s_carry += s_scan[t];
+        __syncthreads();
+    }
+    __syncthreads();
+    if (t == 0) {
+        if (!stop && p < log_cap) {
+            PassRec& R = log[p];
+            R.pending = pend; R.demand = dem; R.hot_pending = hp; R.pushed_before = ctrl->pushed;
+            for (int k = 0; k < MAXM; k++) R.rsum[k] = ctrl->rsum[k];
+            R.n_list = s_nl; R.n_range = s_nr;
+        }
+        ctrl->items = stop ? 0 : s_carry;
+        if (stop) ctrl->done = 1; else ctrl->pass = p + 1;
+        *hub_cnt = 0;
+        ctrl->hotpend = 0;
+        if (!stop) for (int k = 0; k < MAXM; k++) ctrl->rsum[k] = 0;
+        if (use_cond) cudaGraphSetConditional(cond, stop ? 0u : 1u);
+    }
+    // zero the demand table for the next snapshot (after everyone read it)
+    __syncthreads();
+    if (!stop) for (int c = t; c < 2 * nc; c += blockDim.x) cnt[c] = 0;
+}
+
+template <int SRC>
+__device__ __forceinline__ bool get_item(const PushArgs& a, long long t, int& v, const int*& nb, ull& deg) {
+    if constexpr (SRC == SRC_TABLE) {
+        if (t >= (long long)a.wt_prefix[a.nc]) return false;
+        int lo = 0, hi = a.nc - 1;  // chunk c with prefix[c] <= t < prefix[c+1]
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if ((long long)a.wt_prefix[mid] <= t) lo = mid; else hi = mid - 1;
+        }
+        const unsigned i = (unsigned)(t - a.wt_prefix[lo]);
+        if (a.wt_type[lo] == WT_LIST) v = a.list[a.cv0[lo] + i];
+        else {
+            v = a.cv0[lo] + (int)i;
+            if (a.hot && bit_of(a.hot, v)) return false;
+        }
+        const ull b = a.idx[v];
+        deg = a.idx[v + 1] - b;
+        nb = a.cache + b;
+        return true;
+    } else if constexpr (SRC == SRC_CHUNK) {
+        if (t >= (long long)a.ccount) return false;
+        if (a.ctype == WT_LIST) v = a.list[a.cv_0 + (int)t];
+        else {
+            v = a.cv_0 + (int)t;
+            if (a.hot && bit_of(a.hot, v)) return false;
+        }
+        const ull b = a.idx[v];
+        deg = a.idx[v + 1] - b;
+        nb = a.ebase + (b - a.e0);
+        return true;
+    } else if constexpr (SRC == SRC_GATHER) {
+        if (t >= (long long)a.gk) return false;
+        v = a.vids[t];
+        const ull b = a.off[t];
+        deg = a.off[t + 1] - b;
+        nb = a.gedges + b;
+        return true;
+    } else {
+        if (t >= (long long)a.ctrl->hcount) return false;
+        const int j = a.hlist[t];
+        v = a.hids[j];
+        const ull b = a.hoff[j];
+        deg = a.hoff[j + 1] - b;
+        nb = a.hedges + b;
+        return true;
+    }
+}
+
+template <int SRC>
+__device__ __forceinline__ long long item_total(const PushArgs& a) {
+    if constexpr (SRC == SRC_TABLE) return a.wt_prefix[a.nc];
+    else if constexpr (SRC == SRC_CHUNK) return a.ccount;
+    else if constexpr (SRC == SRC_GATHER) return a.gk;
+    else return a.ctrl->hcount;
+}
+
+// Push kernel (persistent grid, warp tiles of 32 items). Each lane takes one
+// item's residual (the push-time re-check and exchange of
+// src/excent.cu:109-112), then the warp dispatches by degree: lists of <= 32
+// entries are scattered edge-balanced across the warp (lane j handles the
+// j-th entry of the tile's concatenated lists), lists up to 2048 entries by
+// the whole warp with 128-bit index loads, longer lists are queued as
+// 2048-entry hub segments for k_hub. Residuals are added with red.global
+// (a float4 reduction per edge carries every measure of an `all` run).
+template <int L, int SRC>
+__global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
+    typedef typename Lane<L>::T T;
+    T* x = reinterpret_cast<T*>(a.x);
+    T* r = reinterpret_cast<T*>(a.r);
+    __shared__ const int* s_nb[BLOCK / 32][32];
+    __shared__ unsigned s_ex[BLOCK / 32][32];
+    __shared__ T s_p[BLOCK / 32][32];
+    __shared__ ull s_pushed[BLOCK / 32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const long long total = item_total<SRC>(a);
+    ull pushed = 0;
+    for (long long tile = gw; tile * 32 < total; tile += nwarps) {
+        int v = 0;
+        const int* nb = nullptr;
+        ull deg = 0;
+        T p{};
+        bool act = false;
+        if (get_item<SRC>(a, tile * 32 + lane, v, nb, deg)) {
+            p = take(x, r, v, deg, a.M);
+            act = nonzero(p) && deg > 0;
+        }
+        if (act) pushed += deg;
+        const bool small = act && deg <= SMALL_MAX;
+        const bool medium = act && deg > SMALL_MAX && deg <= HUB_MIN;
+        const bool large = act && deg > HUB_MIN;
+        if (large) {
+            const unsigned nseg = (unsigned)((deg + HUB_SEG - 1) / HUB_SEG);
+            const ull base = atomicAdd(a.hub_cnt, (ull)nseg);
+            if (base + nseg <= a.hub_cap) {
+                HubSeg* q = a.hubq + base;
+                for (unsigned s = 0; s < nseg; s++) {
+                    HubSeg h;
+                    h.nb = nb + (ull)s * HUB_SEG;
+                    h.len = (unsigned)min((ull)HUB_SEG, deg - (ull)s * HUB_SEG);
+                    h.pad = 0;
+                    if constexpr (L == 1) h.p = make_float4(p, 0.f, 0.f, 0.f); else h.p = p;
+                    q[s] = h;
+                }
+            } else {
+                atomicExch(&a.ctrl->err, 1);
+            }
+        }
+        uint32_t mm = __ballot_sync(FULL, medium);
+        while (mm) {
+            const int sl = __ffs(mm) - 1;
+            mm &= mm - 1;
+            const int* nbm = shfl_ptr(nb, sl);
+            const unsigned dm = __shfl_sync(FULL, (unsigned)deg, sl);
+            const T pm = shfl(p, sl);
+            warp_scatter(r, nbm, dm, pm, lane);
+        }
+        const unsigned ds = small ? (unsigned)deg : 0u;
+        const unsigned incl = warp_incl_scan(ds, lane);
+        const unsigned tot = __shfl_sync(FULL, incl, 31);
+        if (tot) {
+            s_nb[wib][lane] = nb;
+            s_ex[wib][lane] = incl - ds;
+            if (small) s_p[wib][lane] = p;
+            __syncwarp();
+            for (unsigned j0 = 0; j0 < tot; j0 += 32) {
+                const unsigned j = j0 + lane;
+                int lo = 0;
+#pragma unroll
+                for (int step = 16; step > 0; step >>= 1) {
+                    const unsigned val = __shfl_sync(FULL, incl, lo + step - 1);
+                    if (val <= j) lo += step;
+                }
+                if (j < tot) {
+                    const int u = ld_edge(s_nb[wib][lo] + (j - s_ex[wib][lo]));
+                    red_add(r, u, s_p[wib][lo]);
+                }
+            }
+            __syncwarp();
+        }
+    }
+    pushed = warp_sum(pushed);
+    if (lane == 0) s_pushed[wib] = pushed;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ull t = 0;
+        for (int i = 0; i < BLOCK / 32; i++) t += s_pushed[i];
+        if (t) atomicAdd(&a.ctrl->pushed, t);
+    }
+}
+
+// Hub segments queued by k_push: one warp per 2048-entry segment.
+template <int L>
+__global__ void __launch_bounds__(BLOCK) k_hub(void* rv, const HubSeg* q, const ull* hub_cnt, ull cap) {
+    typedef typename Lane<L>::T T;
+    T* r = reinterpret_cast<T*>(rv);
+    const int lane = threadIdx.x & 31;
+    const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    ull cnt = *hub_cnt;
+    if (cnt > cap) cnt = cap;
+    for (long long s = gw; s < (long long)cnt; s += nwarps) {
+        const HubSeg h = q[s];
+        T p;
+        if constexpr (L == 1) p = h.p.x; else p = h.p;
+        warp_scatter(r, h.nb, h.len, p, lane);
+    }
+}
+
+// Pending hot vertices among hot ids [lo, hi) at launch time, appended with
+// one global atomic per block (src/excent.cu:178-182).
+template <int L>
+__global__ void __launch_bounds__(BLOCK) k_compact_hot(int lo, int hi, const int* hids, const void* rv, DevMeasures M,
+                                                       int* out, Ctrl* ctrl) {
+    typedef typename Lane<L>::T T;
+    const T* r = reinterpret_cast<const T*>(rv);
+    __shared__ unsigned s_cnt, s_base;
+    __shared__ unsigned s_w[BLOCK / 32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    for (long long i0 = lo + (long long)blockIdx.x * BLOCK; i0 < hi; i0 += (long long)gridDim.x * BLOCK) {
+        const long long i = i0 + threadIdx.x;
+        const bool p = i < hi && pending_of(r[hids[i]], M);
+        const uint32_t b = __ballot_sync(FULL, p);
+        if (threadIdx.x == 0) s_cnt = 0;
+        __syncthreads();
+        if (lane == 0) s_w[wib] = atomicAdd(&s_cnt, (unsigned)__popc(b));
+        __syncthreads();
+        if (threadIdx.x == 0) s_base = s_cnt ? atomicAdd(&ctrl->hcount, s_cnt) : 0;
+        __syncthreads();
+        if (p) out[s_base + s_w[wib] + __popc(b & ((1u << lane) - 1u))] = (int)i;
+        __syncthreads();
+    }
+}
+
+// Pass 0: copy the lists of hot ids [lo, hi) out of a chunk staged at src
+// (edges from e0), one warp per vertex (src/excent.cu:211-220).
+__global__ void k_fill_hot(int lo, int hi, const int* hids, const ull* hoff, const ull* idx, ull e0, const int* src,
+                           int* hedges) {
+    const long long w = lo + ((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (w >= hi) return;
+    const int* from = src + (idx[hids[w]] - e0);
+    int* to = hedges + hoff[w];
+    for (ull i = lane, d = hoff[w + 1] - hoff[w]; i < d; i += 32) to[i] = from[i];
+}
+
+// Measure i of a float4 layout into a float array, for readback.
+__global__ void k_extract(int n, const float4* s, int i, float* out) {
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
+        const float4 q = s[v];
+        out[v] = i == 0 ? q.x : i == 1 ? q.y : q.z;
+    }
+}
+__global__ void k_insert(int n, float4* s, int i, const float* in) {
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
+        float4 q = s[v];
+        if (i == 0) q.x = in[v]; else if (i == 1) q.y = in[v]; else q.z = in[v];
+        s[v] = q;
+    }
+}
+
+}  // namespace excent
+
+using namespace excent;
+
+// ------------------------------------------------------------------ engine
+
+struct Slot {
+    int* h_edges = nullptr; int* d_edges = nullptr;
+    int* h_vids = nullptr; int* d_vids = nullptr;
+    ull* h_off = nullptr; ull* d_off = nullptr;
+    cudaStream_t st = nullptr;
+    cudaEvent_t done = nullptr;
+    bool busy = false;
+};
+
+struct excent_engine {
+    int dev = 0, sms = 0;
+    int n = 0;
+    ull m = 0;
+    int nm = 0, L = 1;
+    excent_measures meas{};
+    DevMeasures M{};
+    int nc = 0;
+    std::vector<int> cv0;
+    std::vector<ull> ce;
+    std::vector<uint8_t> loaded;
+    // device state
+    ull* d_idx = nullptr;
+    void* d_x = nullptr;
+    void* d_r = nullptr;
+    uint32_t* d_bitmap = nullptr;
+    ull* d_cnt = nullptr;
+    int* d_cv0 = nullptr;
+    int* d_list = nullptr;
+    Ctrl* d_ctrl = nullptr;
+    uint8_t* d_cmode = nullptr;
+    uint8_t* d_wt_type = nullptr;
+    unsigned* d_wt_prefix = nullptr;
+    HubSeg* d_hubq[3] = {nullptr, nullptr, nullptr};  // per stream: main, slot 0, slot 1
+    ull hub_cap[3] = {0, 0, 0};
+    ull* d_hubcnt = nullptr;                           // 3 counters
+    bool hot_skip = false;                             // this pass skips cached high-degree vertices
+    PassRec* d_log = nullptr;
+    int log_cap = 0;
+    uint16_t* d_trace = nullptr;
+    bool trace_on = false;
+    float* d_tmp = nullptr;  // n floats for readback of the float4 layout
+    int* d_cache = nullptr;
+    ull cache_edges = 0;
+    // hot cache
+    int nh = 0;
+    int* d_hids = nullptr; ull* d_hoff = nullptr; int* d_hedges = nullptr; uint32_t* d_hot = nullptr;
+    int* d_hlist = nullptr;
+    // pinned host mirrors
+    ull* h_cnt = nullptr;
+    Ctrl* h_ctrl = nullptr;
+    uint8_t* h_wt_type = nullptr;
+    unsigned* h_wt_prefix = nullptr;
+    // streams
+    cudaStream_t s_main = nullptr;
+    Slot slot[2];
+    bool slots_ok = false, zc = false;
+    ull max_chunk_edges = 0;
+    int max_chunk_verts = 0;
+    // graph
+    cudaGraphExec_t gexec = nullptr;
+    cudaGraph_t graph = nullptr;
+    int graph_max_passes = -1;
+    double graph_list_frac = -1;
+    // per-kernel timing of the host-driven device solve (excent_engine_profile)
+    bool prof = false;
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    double prof_ms[4] = {0, 0, 0, 0};  // snapshot, plan, push, hub
+    ull prof_passes = 0;
+    // launch grids
+    int grid_push = 0, grid_snap = 0, groups_per_warp = 1;
+    ull launches = 0;
+    ull n_list = 0, n_range = 0;
+};
+
+// Device pointers and launch parameters are baked into the solve graph:
+// any reallocation or option change drops it.
+static void invalidate_graph(excent_engine* e) {
+    if (e->gexec) { cudaGraphExecDestroy(e->gexec); e->gexec = nullptr; }
+    if (e->graph) { cudaGraphDestroy(e->graph); e->graph = nullptr; }
+}
+
+static int free_engine(excent_engine* e) {
+    if (!e) return EXCENT_OK;
+    cudaSetDevice(e->dev);
+    cudaDeviceSynchronize();
+    if (e->gexec) cudaGraphExecDestroy(e->gexec);
+    if (e->graph) cudaGraphDestroy(e->graph);
+    void* dptrs[] = {e->d_idx, e->d_x, e->d_r, e->d_bitmap, e->d_cnt, e->d_cv0, e->d_list, e->d_ctrl, e->d_cmode,
+                     e->d_wt_type, e->d_wt_prefix, e->d_hubq[0], e->d_hubq[1], e->d_hubq[2], e->d_hubcnt, e->d_log, e->d_trace, e->d_tmp, e->d_cache,
+                     e->d_hids, e->d_hoff, e->d_hedges, e->d_hot, e->d_hlist};
+    for (void* p : dptrs) if (p) cudaFree(p);
+    void* hptrs[] = {e->h_cnt, e->h_ctrl, e->h_wt_type, e->h_wt_prefix};
+    for (void* p : hptrs) if (p) cudaFreeHost(p);
+    for (Slot& s : e->slot) {
+        if (s.h_edges) cudaFreeHost(s.h_edges);
+        if (s.h_vids) cudaFreeHost(s.h_vids);
+        if (s.h_off) cudaFreeHost(s.h_off);
+        if (!e->zc) {
+            if (s.d_edges) cudaFree(s.d_edges);
+            if (s.d_vids) cudaFree(s.d_vids);
+            if (s.d_off) cudaFree(s.d_off);
+        }
+        if (s.st) cudaStreamDestroy(s.st);
+        if (s.done) cudaEventDestroy(s.done);
+    }
+    for (cudaEvent_t ev : e->ev) if (ev) cudaEventDestroy(ev);
+    if (e->s_main) cudaStreamDestroy(e->s_main);
+    delete e;
+    return EXCENT_OK;
+}
+
+#define EX_ALLOC(ptr, bytes) do { if (cudaMalloc((void**)&(ptr), (bytes)) != cudaSuccess) { cudaGetLastError(); \
+    ::excent::set_error("device allocation of %llu bytes failed (%s)", (ull)(bytes), #ptr); return EXCENT_ERR_NOMEM; } } while (0)
+#define EX_HALLOC(ptr, bytes) do { if (cudaMallocHost((void**)&(ptr), (bytes)) != cudaSuccess) { cudaGetLastError(); \
+    ::excent::set_error("pinned allocation of %llu bytes failed (%s)", (ull)(bytes), #ptr); return EXCENT_ERR_NOMEM; } } while (0)
+
+static int engine_setup(excent_engine* e, int device, int n, ull m, const excent_measures* ms, int nc,
+                        const int* chunk_v0, const ull* chunk_e) {
+    EX_CUDA(cudaSetDevice(device));
+    e->dev = device;
+    EX_CUDA(cudaDeviceGetAttribute(&e->sms, cudaDevAttrMultiProcessorCount, device));
+    e->n = n; e->m = m; e->nm = ms->nm; e->L = ms->nm == 1 ? 1 : 4;
+    e->meas = *ms;
+    e->M.nm = ms->nm;
+    for (int k = 0; k < MAXM; k++) {
+        e->M.eps[k] = k < ms->nm ? ms->eps[k] : 0.f;
+        e->M.scale[k] = k < ms->nm ? ms->scale[k] : 0.f;
+        e->M.divdeg[k] = k < ms->nm ? ms->divdeg[k] : 0;
+    }
+    e->nc = nc;
+    e->cv0.assign(chunk_v0, chunk_v0 + nc);
+    e->ce.assign(chunk_e, chunk_e + nc + 1);
+    e->loaded.assign(nc, 0);
+    for (int c = 0; c < nc; c++) {
+        const int v1 = c + 1 < nc ? chunk_v0[c + 1] : n;
+        EX_CHECK_ARG(chunk_v0[c] >= 0 && chunk_v0[c] < v1 && v1 <= n, "chunk %d has an empty or bad range", c);
+        EX_CHECK_ARG(chunk_e[c] <= chunk_e[c + 1], "chunk %d has bad edge bounds", c);
+        e->max_chunk_verts = std::max(e->max_chunk_verts, v1 - chunk_v0[c]);
+        e->max_chunk_edges = std::max(e->max_chunk_edges, chunk_e[c + 1] - chunk_e[c]);
+    }
+    EX_CHECK_ARG(chunk_v0[0] == 0 && chunk_e[0] == 0 && chunk_e[nc] == m, "chunks must cover the graph");
+    EX_CUDA(cudaStreamCreateWithFlags(&e->s_main, cudaStreamNonBlocking));
+    const size_t words = ((size_t)n + 31) / 32;
+    const size_t vbytes = (size_t)n * (e->L == 1 ? sizeof(float) : sizeof(float4));
+    EX_ALLOC(e->d_idx, ((size_t)n + 1) * sizeof(ull));
+    EX_ALLOC(e->d_x, vbytes);
+    EX_ALLOC(e->d_r, vbytes);
+    EX_ALLOC(e->d_bitmap, words * sizeof(uint32_t));
+    EX_ALLOC(e->d_cnt, 2 * (size_t)nc * sizeof(ull));
+    EX_ALLOC(e->d_cv0, (size_t)nc * sizeof(int));
+    EX_ALLOC(e->d_list, (size_t)n * sizeof(int));
+    EX_ALLOC(e->d_ctrl, sizeof(Ctrl));
+    EX_ALLOC(e->d_cmode, (size_t)nc);
+    EX_ALLOC(e->d_wt_type, (size_t)nc);
+    EX_ALLOC(e->d_wt_prefix, ((size_t)nc + 1) * sizeof(unsigned));
+    e->hub_cap[0] = 2 * (m / HUB_SEG) + 64;
+    EX_ALLOC(e->d_hubq[0], e->hub_cap[0] * sizeof(HubSeg));
+    EX_ALLOC(e->d_hubcnt, 3 * sizeof(ull));
+    e->log_cap = 1 << 16;
+    EX_ALLOC(e->d_log, (size_t)e->log_cap * sizeof(PassRec));
+    if (e->L == 4) EX_ALLOC(e->d_tmp, (size_t)n * sizeof(float));
+    EX_HALLOC(e->h_cnt, 2 * (size_t)nc * sizeof(ull));
+    EX_HALLOC(e->h_ctrl, sizeof(Ctrl));
+    EX_HALLOC(e->h_wt_type, (size_t)nc);
+    EX_HALLOC(e->h_wt_prefix, ((size_t)nc + 1) * sizeof(unsigned));
+    EX_CUDA(cudaMemcpy(e->d_cv0, chunk_v0, (size_t)nc * sizeof(int), cudaMemcpyHostToDevice));
+    EX_CUDA(cudaMemset(e->d_ctrl, 0, sizeof(Ctrl)));
+    EX_CUDA(cudaMemset(e->d_cnt, 0, 2 * (size_t)nc * sizeof(ull)));
+    EX_CUDA(cudaMemset(e->d_cmode, 0, (size_t)nc));
+    EX_CUDA(cudaMemset(e->d_hubcnt, 0, 3 * sizeof(ull)));
+    int occ = 0;
+    if (e->L == 1) EX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_push<1, SRC_TABLE>, BLOCK, 0));
+    else EX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_push<4, SRC_TABLE>, BLOCK, 0));
+    e->grid_push = e->sms * std::max(1, occ);
+    int occs = 0;
+    if (e->L == 1) EX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occs, k_snapshot<1>, BLOCK, 0));
+    else EX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occs, k_snapshot<4>, BLOCK, 0));
+    const long long groups = ((long long)words + SNAP_GROUP - 1) / SNAP_GROUP;
+    const long long max_warps = (long long)e->sms * std::max(1, occs) * (BLOCK / 32);
+    e->groups_per_warp = (int)std::max(1LL, (groups + max_warps - 1) / max_warps);
+    const long long warps = (groups + e->groups_per_warp - 1) / e->groups_per_warp;
+    e->grid_snap = (int)std::max(1LL, (warps + BLOCK / 32 - 1) / (BLOCK / 32));
+    return EXCENT_OK;
+}
+
+extern "C" int excent_measures_make(excent_measures* out, const char* measure, double alpha, double beta,
+                                    double lambda, double eps_pr, double eps_katz, double eps_ev) {
+    EX_CHECK_ARG(out && measure, "null argument");
+    excent_measures M{};
+    int kinds[3], nm = 0;
+    if (!strcmp(measure, "pr")) kinds[nm++] = EXCENT_PR;
+    else if (!strcmp(measure, "katz")) kinds[nm++] = EXCENT_KATZ;
+    else if (!strcmp(measure, "ev")) kinds[nm++] = EXCENT_EV;
+    else if (!strcmp(measure, "all")) { kinds[nm++] = EXCENT_PR; kinds[nm++] = EXCENT_KATZ; kinds[nm++] = EXCENT_EV; }
+    else EX_FAIL(EXCENT_ERR_ARG, "--measure must be pr, katz, ev or all");
+    for (int i = 0; i < nm; i++) {
+        if (kinds[i] == EXCENT_KATZ && (alpha <= 0 || eps_katz <= 0)) EX_FAIL(EXCENT_ERR_ARG, "katz needs --alpha and --eps-katz");
+        if (kinds[i] == EXCENT_EV && (lambda <= 0 || eps_ev <= 0)) EX_FAIL(EXCENT_ERR_ARG, "ev needs --lambda and --eps-ev");
+    }
+    M.nm = nm;
+    for (int i = 0; i < nm; i++) {
+        const int k = kinds[i];
+        M.kind[i] = k;
+        M.eps[i] = (float)(k == EXCENT_PR ? eps_pr : k == EXCENT_KATZ ? eps_katz : eps_ev);
+        M.scale[i] = (float)(k == EXCENT_PR ? 0.85f : k == EXCENT_KATZ ? alpha : 1.0 / lambda);
+        M.divdeg[i] = k == EXCENT_PR;
+    }
+    M.beta = beta;
+    M.lambda = lambda;
+    *out = M;
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_create(int device, int n, unsigned long long m, const excent_measures* measures, int nc,
+                                    const int* chunk_v0, const unsigned long long* chunk_e, excent_engine** out) {
+    EX_CHECK_ARG(out && measures && chunk_v0 && chunk_e, "null argument");
+    EX_CHECK_ARG(n >= 1, "n must be >= 1");
+    EX_CHECK_ARG(nc >= 1 && nc <= n, "bad chunk count %d", nc);
+    EX_CHECK_ARG(measures->nm >= 1 && measures->nm <= 3, "nm must be 1..3");
+    *out = nullptr;
+    excent_engine* e = new excent_engine();
+    const int rc = engine_setup(e, device, n, m, measures, nc, chunk_v0, chunk_e);
+    if (rc != EXCENT_OK) {
+        std::string msg = excent::get_error();
+        free_engine(e);
+        excent::set_error("%s", msg.c_str());
+        return rc;
+    }
+    *out = e;
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_destroy(excent_engine* e) { return free_engine(e); }
+
+extern "C" int excent_engine_upload_offsets(excent_engine* e, const unsigned long long* idx, unsigned long long v0,
+                                            unsigned long long count) {
+    EX_CHECK_ARG(e && idx, "null argument");
+    EX_CHECK_ARG(v0 + count <= (ull)e->n + 1, "offsets out of range");
+    EX_CUDA(cudaSetDevice(e->dev));
+    EX_CUDA(cudaMemcpyAsync(e->d_idx + v0, idx, count * sizeof(ull), cudaMemcpyHostToDevice, e->s_main));
+    EX_CUDA(cudaStreamSynchronize(e->s_main));
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_upload_device(excent_engine* e, const unsigned long long* d_idx, const int32_t* d_adj) {
+    EX_CHECK_ARG(e && d_idx && (d_adj || e->m == 0), "null argument");
+    EX_CUDA(cudaSetDevice(e->dev));
+    EX_CUDA(cudaMemcpyAsync(e->d_idx, d_idx, ((size_t)e->n + 1) * sizeof(ull), cudaMemcpyDeviceToDevice, e->s_main));
+    if (e->cache_edges != e->m) EX_TRY(excent_engine_reserve_cache(e, e->m));
+    if (e->m) EX_CUDA(cudaMemcpyAsync(e->d_cache, d_adj, e->m * sizeof(int), cudaMemcpyDeviceToDevice, e->s_main));
+    EX_CUDA(cudaStreamSynchronize(e->s_main));
+    std::fill(e->loaded.begin(), e->loaded.end(), 1);
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_reserve_cache(excent_engine* e, unsigned long long edges) {
+    EX_CHECK_ARG(e && edges <= e->m, "bad cache size");
+    EX_CUDA(cudaSetDevice(e->dev));
+    invalidate_graph(e);
+    EX_CUDA(cudaDeviceSynchronize());
+    if (e->d_cache) { cudaFree(e->d_cache); e->d_cache = nullptr; e->cache_edges = 0; }
+    if (edges == 0) return EXCENT_OK;
+    if (cudaMalloc((void**)&e->d_cache, edges * sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        e->d_cache = nullptr;
+        EX_FAIL(EXCENT_ERR_NOMEM, "edge cache of %llu edges does not fit", edges);
+    }
+    e->cache_edges = edges;
+    std::fill(e->loaded.begin(), e->loaded.end(), 0);
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_load_cache(excent_engine* e, unsigned long long e0, unsigned long long e1,
+                                        const int32_t* edges) {
+    EX_CHECK_ARG(e && edges && e0 <= e1 && e1 <= e->cache_edges, "edges [%llu, %llu) outside the cache", e0, e1);
+    EX_CUDA(cudaSetDevice(e->dev));
+    EX_CUDA(cudaMemcpyAsync(e->d_cache + e0, edges, (e1 - e0) * sizeof(int), cudaMemcpyHostToDevice, e->s_main));
+    EX_CUDA(cudaStreamSynchronize(e->s_main));
+    for (int c = 0; c < e->nc; c++) if (e->ce[c] >= e0 && e->ce[c + 1] <= e1) e->loaded[c] = 1;
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_set_loaded(excent_engine* e, int c, int loaded) {
+    EX_CHECK_ARG(e && c >= 0 && c < e->nc, "bad chunk");
+    EX_CHECK_ARG(!loaded || e->ce[c + 1] <= e->cache_edges, "chunk %d is not inside the edge cache", c);
+    e->loaded[c] = loaded ? 1 : 0;
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_trace(excent_engine* e, int enable) {
+    EX_CHECK_ARG(e, "null engine");
+    EX_CUDA(cudaSetDevice(e->dev));
+    invalidate_graph(e);
+    if (enable && !e->d_trace) EX_ALLOC(e->d_trace, (size_t)e->n * sizeof(uint16_t));
+    e->trace_on = enable != 0;
+    if (e->d_trace) EX_CUDA(cudaMemset(e->d_trace, 0, (size_t)e->n * sizeof(uint16_t)));
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_read_trace(excent_engine* e, uint16_t* out) {
+    EX_CHECK_ARG(e && out && e->d_trace, "trace not enabled");
+    EX_CUDA(cudaSetDevice(e->dev));
+    EX_CUDA(cudaStreamSynchronize(e->s_main));
+    EX_CUDA(cudaMemcpy(out, e->d_trace, (size_t)e->n * sizeof(uint16_t), cudaMemcpyDeviceToHost));
+    return EXCENT_OK;
+}
+
+static int init_state(excent_engine* e) {
+    const excent_measures& ms = e->meas;
+    const int g = e->sms * 8;
+    if (e->L == 1)
+        k_init<1><<<g, BLOCK, 0, e->s_main>>>(e->n, e->d_idx, (float*)e->d_x, (float*)e->d_r, e->nm,
+                                               ms.kind[0], 0, 0, (float)ms.beta, (float)ms.lambda);
+    else
+        k_init<4><<<g, BLOCK, 0, e->s_main>>>(e->n, e->d_idx, (float4*)e->d_x, (float4*)e->d_r, e->nm,
+                                               ms.kind[0], ms.kind[1], ms.kind[2], (float)ms.beta, (float)ms.lambda);
+    e->launches++;
+    EX_CUDA(cudaGetLastError());
+    EX_CUDA(cudaMemsetAsync(e->d_ctrl, 0, sizeof(Ctrl), e->s_main));
+    EX_CUDA(cudaMemsetAsync(e->d_hubcnt, 0, 3 * sizeof(ull), e->s_main));
+    EX_CUDA(cudaMemsetAsync(e->d_cnt, 0, 2 * (size_t)e->nc * sizeof(ull), e->s_main));
+    e->hot_skip = false;
+    if (e->d_trace && e->trace_on) EX_CUDA(cudaMemsetAsync(e->d_trace, 0, (size_t)e->n * sizeof(uint16_t), e->s_main));
+    e->n_list = e->n_range = 0;
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_init(excent_engine* e) {
+    EX_CHECK_ARG(e, "null engine");
+    EX_CUDA(cudaSetDevice(e->dev));
+    EX_TRY(init_state(e));
+    EX_CUDA(cudaStreamSynchronize(e->s_main));
+    return EXCENT_OK;
+}
+
+static SnapArgs snap_args(excent_engine* e, bool use_hot) {
+    SnapArgs a{};
+    a.n = e->n; a.nc = e->nc; a.words = (int)(((size_t)e->n + 31) / 32); a.groups_per_warp = e->groups_per_warp;
+    a.r = e->d_r; a.M = e->M; a.idx = e->d_idx; a.cv0 = e->d_cv0;
+    a.hot = use_hot ? e->d_hot : nullptr;
+    a.bitmap = e->d_bitmap; a.cnt = e->d_cnt; a.list = e->d_list;
+    a.trace = e->trace_on ? e->d_trace : nullptr;
+    a.ctrl = e->d_ctrl;
+    return a;
+}
+
+static void launch_snapshot(excent_engine* e, bool use_hot, cudaStream_t st) {
+    SnapArgs a = snap_args(e, use_hot);
+    if (e->L == 1) k_snapshot<1><<<e->grid_snap, BLOCK, 0, st>>>(a);
+    else k_snapshot<4><<<e->grid_snap, BLOCK, 0, st>>>(a);
+    e->launches++;
+}
+
+extern "C" int excent_engine_snapshot(excent_engine* e, int use_hot, unsigned long long* cnt,
+                                      unsigned long long* hotpend, double* rsum) {
+    EX_CHECK_ARG(e, "null engine");
+    EX_CHECK_ARG(!use_hot || e->d_hot, "hot snapshot without a hot cache");
+    EX_CUDA(cudaSetDevice(e->dev));
+    EX_CUDA(cudaMemsetAsync(e->d_cnt, 0, 2 * (size_t)e->nc * sizeof(ull), e->s_main));
+    EX_CUDA(cudaMemsetAsync(&e->d_ctrl->hotpend, 0, sizeof(ull), e->s_main));
+    EX_CUDA(cudaMemsetAsync(e->d_ctrl->rsum, 0, sizeof(double) * MAXM, e->s_main));
+    e->hot_skip = use_hot != 0;
+    launch_snapshot(e, use_hot != 0, e->s_main);
+    EX_CUDA(cudaGetLastError());
+    EX_CUDA(cudaMemcpyAsync(e->h_cnt, e->d_cnt, 2 * (size_t)e->nc * sizeof(ull), cudaMemcpyDeviceToHost, e->s_main));
+    EX_CUDA(cudaMemcpyAsync(e->h_ctrl, e->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, e->s_main));
+    EX_CUDA(cudaStreamSynchronize(e->s_main));
+    if (cnt) memcpy(cnt, e->h_cnt, 2 * (size_t)e->nc * sizeof(ull));
+    if (hotpend) *hotpend = e->h_ctrl->hotpend;
+    if (rsum) for (int k = 0; k < e->nm; k++) rsum[k] = e->h_ctrl->rsum[k];
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_bitmap(excent_engine* e, uint32_t* words) {
+    EX_CHECK_ARG(e && words, "null argument");
+    EX_CUDA(cudaSetDevice(e->dev));
+    EX_CUDA(cudaStreamSynchronize(e->s_main));
+    EX_CUDA(cudaMemcpy(words, e->d_bitmap, (((size_t)e->n + 31) / 32) * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_chunk_list(excent_engine* e, int c, int32_t* ids, unsigned int* k) {
+    EX_CHECK_ARG(e && ids && k && c >= 0 && c < e->nc, "bad argument");
+    EX_CUDA(cudaSetDevice(e->dev));
+    EX_CUDA(cudaStreamSynchronize(e->s_main));
+    ull cnt = 0;
+    EX_CUDA(cudaMemcpy(&cnt, e->d_cnt + 2 * c, sizeof(ull), cudaMemcpyDeviceToHost));
+    *k = (unsigned)cnt;
+    if (cnt) EX_CUDA(cudaMemcpy(ids, e->d_list + e->cv0[c], cnt * sizeof(int), cudaMemcpyDeviceToHost));
+    return EXCENT_OK;
+}
+
+static PushArgs push_args(excent_engine* e, int q) {
+    PushArgs a{};
+    a.x = e->d_x; a.r = e->d_r; a.M = e->M; a.idx = e->d_idx; a.hot = nullptr;
+    a.nc = e->nc; a.cv0 = e->d_cv0; a.wt_type = e->d_wt_type; a.wt_prefix = e->d_wt_prefix; a.list = e->d_list;
+    a.cache = e->d_cache;
+    a.hids = e->d_hids; a.hoff = e->d_hoff; a.hedges = e->d_hedges; a.hlist = e->d_hlist;
+    a.hubq = e->d_hubq[q]; a.hub_cap = e->hub_cap[q]; a.hub_cnt = e->d_hubcnt + q; a.ctrl = e->d_ctrl;
+    return a;
+}
+
+template <int SRC>
+static void launch_push(excent_engine* e, const PushArgs& a, int grid, cudaStream_t st) {
+    if (e->L == 1) {
+        k_push<1, SRC><<<grid, BLOCK, 0, st>>>(a);
+        k_hub<1><<<e->grid_push, BLOCK, 0, st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap);
+    } else {
+        k_push<4, SRC><<<grid, BLOCK, 0, st>>>(a);
+        k_hub<4><<<e->grid_push, BLOCK, 0, st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap);
+    }
+    e->launches += 2;
+}
+
+static int grid_for(excent_engine* e, ull items) {
+    const ull warps = (items + 31) / 32;
+    const ull blocks = (warps + BLOCK / 32 - 1) / (BLOCK / 32);
+    return (int)std::max<ull>(1, std::min<ull>(blocks, (ull)e->grid_push));
+}
+
+extern "C" int excent_engine_push_cached(excent_engine* e, const unsigned char* mode, const unsigned long long* cnt,
+                                         double list_frac) {
+    EX_CHECK_ARG(e && mode && cnt, "null argument");
+    EX_CHECK_ARG(e->d_cache, "no edge cache");
+    EX_CUDA(cudaSetDevice(e->dev));
+    unsigned total = 0;
+    e->h_wt_prefix[0] = 0;
+    for (int c = 0; c < e->nc; c++) {
+        uint8_t ty = WT_NONE;
+        unsigned items = 0;
+        if (mode[c] == 1 && cnt[2 * c] > 0) {
+            EX_CHECK_ARG(e->ce[c + 1] <= e->cache_edges, "chunk %d is not in the edge cache", c);
+            const int nv = (c + 1 < e->nc ? e->cv0[c + 1] : e->n) - e->cv0[c];
+            if ((double)cnt[2 * c] < list_frac * nv) { ty = WT_LIST; items = (unsigned)cnt[2 * c]; e->n_list++; }
+            else { ty = WT_RANGE; items = (unsigned)nv; e->n_range++; }
+        }
+        e->h_wt_type[c] = ty;
+        total += items;
+        e->h_wt_prefix[c + 1] = total;
+    }
+    if (total == 0) return EXCENT_OK;
+    EX_CUDA(cudaMemcpyAsync(e->d_wt_type, e->h_wt_type, e->nc, cudaMemcpyHostToDevice, e->s_main));
+    EX_CUDA(cudaMemcpyAsync(e->d_wt_prefix, e->h_wt_prefix, ((size_t)e->nc + 1) * sizeof(unsigned),
+                            cudaMemcpyHostToDevice, e->s_main));
+    EX_CUDA(cudaMemsetAsync(e->d_hubcnt, 0, sizeof(ull), e->s_main));
+    PushArgs a = push_args(e, 0);
+    a.hot = e->hot_skip ? e->d_hot : nullptr;
+    launch_push<SRC_TABLE>(e, a, grid_for(e, total), e->s_main);
+    EX_CUDA(cudaGetLastError());
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_slots_create(excent_engine* e, unsigned long long max_chunk_edges, int max_chunk_verts,
+                                          int zero_copy) {
+    EX_CHECK_ARG(e && max_chunk_verts >= 1, "bad argument");
+    EX_CHECK_ARG(!e->slots_ok, "slots already created");
+    EX_CUDA(cudaSetDevice(e->dev));
+    e->zc = zero_copy != 0;
+    for (Slot& s : e->slot) {
+        const size_t eb = std::max<ull>(max_chunk_edges, 1) * sizeof(int);
+        const size_t vb = (size_t)max_chunk_verts * sizeof(int), ob = ((size_t)max_chunk_verts + 1) * sizeof(ull);
+        if (e->zc) {
+            if (cudaHostAlloc((void**)&s.h_edges, eb, cudaHostAllocMapped) != cudaSuccess ||
+                cudaHostAlloc((void**)&s.h_vids, vb, cudaHostAllocMapped) != cudaSuccess ||
+                cudaHostAlloc((void**)&s.h_off, ob, cudaHostAllocMapped) != cudaSuccess) {
+                cudaGetLastError();
+                EX_FAIL(EXCENT_ERR_NOMEM, "mapped staging allocation failed");
+            }
+            EX_CUDA(cudaHostGetDevicePointer((void**)&s.d_edges, s.h_edges, 0));
+            EX_CUDA(cudaHostGetDevicePointer((void**)&s.d_vids, s.h_vids, 0));
+            EX_CUDA(cudaHostGetDevicePointer((void**)&s.d_off, s.h_off, 0));
+        } else {
+            EX_HALLOC(s.h_edges, eb);
+            EX_HALLOC(s.h_vids, vb);
+            EX_HALLOC(s.h_off, ob);
+            EX_ALLOC(s.d_edges, eb);
+            EX_ALLOC(s.d_vids, vb);
+            EX_ALLOC(s.d_off, ob);
+        }
+        EX_CUDA(cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking));
+        EX_CUDA(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
+    }
+    for (int q = 1; q < 3; q++) {
+        e->hub_cap[q] = 2 * (std::max<ull>(max_chunk_edges, 1) / HUB_SEG) + 64;
+        EX_ALLOC(e->d_hubq[q], e->hub_cap[q] * sizeof(HubSeg));
+    }
+    e->max_chunk_edges = std::max<ull>(e->max_chunk_edges, max_chunk_edges);
+    e->slots_ok = true;
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_slot_buffers(excent_engine* e, int s, int32_t** edges, int32_t** vids,
+                                          unsigned long long** off) {
+    EX_CHECK_ARG(e && e->slots_ok && (s == 0 || s == 1), "no such slot");
+    if (edges) *edges = e->slot[s].h_edges;
+    if (vids) *vids = e->slot[s].h_vids;
+    if (off) *off = e->slot[s].h_off;
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_slot_wait(excent_engine* e, int s) {
+    EX_CHECK_ARG(e && e->slots_ok && (s == 0 || s == 1), "no such slot");
+    EX_CUDA(cudaSetDevice(e->dev));
+    Slot& sl = e->slot[s];
+    if (sl.busy) { EX_CUDA(cudaEventSynchronize(sl.done)); sl.busy = false; }
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_push_stream(excent_engine* e, int s, int c, const unsigned long long* cnt,
+                                         double list_frac, int cache_fill, int hlo, int hhi) {
+    EX_CHECK_ARG(e && e->slots_ok && (s == 0 || s == 1) && cnt, "bad argument");
+    EX_CHECK_ARG(c >= 0 && c < e->nc, "bad chunk %d", c);
+    EX_CUDA(cudaSetDevice(e->dev));
+    Slot& sl = e->slot[s];
+    const ull e0 = e->ce[c], e1 = e->ce[c + 1], ne = e1 - e0;
+    EX_CHECK_ARG(ne <= e->max_chunk_edges, "chunk %d larger than the slots", c);
+    const bool to_cache = cache_fill && e->d_cache && e1 <= e->cache_edges;
+    int* dst = to_cache ? e->d_cache + e0 : sl.d_edges;
+    if (!e->zc) { if (ne) EX_CUDA(cudaMemcpyAsync(dst, sl.h_edges, ne * sizeof(int), cudaMemcpyHostToDevice, sl.st)); }
+    else if (to_cache && ne) EX_CUDA(cudaMemcpyAsync(dst, sl.d_edges, ne * sizeof(int), cudaMemcpyDeviceToDevice, sl.st));
+    if (e->d_hedges && hhi > hlo) {
+        const unsigned grid = (unsigned)(((long long)(hhi - hlo) * 32 + BLOCK - 1) / BLOCK);
+        k_fill_hot<<<grid, BLOCK, 0, sl.st>>>(hlo, hhi, e->d_hids, e->d_hoff, e->d_idx, e0, dst, e->d_hedges);
+        e->launches++;
+    }
+    const int v0 = e->cv0[c], nv = (c + 1 < e->nc ? e->cv0[c + 1] : e->n) - v0;
+    const ull k = cnt[2 * c];
+    PushArgs a = push_args(e, 1 + s);
+    a.hot = e->hot_skip ? e->d_hot : nullptr;
+    a.cv_0 = v0; a.ebase = dst; a.e0 = e0;
+    if ((double)k < list_frac * nv) { a.ctype = WT_LIST; a.ccount = (unsigned)k; e->n_list++; }
+    else { a.ctype = WT_RANGE; a.ccount = (unsigned)nv; e->n_range++; }
+    EX_CUDA(cudaMemsetAsync(e->d_hubcnt + 1 + s, 0, sizeof(ull), sl.st));
+    if (a.ccount) launch_push<SRC_CHUNK>(e, a, grid_for(e, a.ccount), sl.st);
+    EX_CUDA(cudaGetLastError());
+    if (to_cache) e->loaded[c] = 1;
+    EX_CUDA(cudaEventRecord(sl.done, sl.st));
+    sl.busy = true;
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_push_gather(excent_engine* e, int s, int k, unsigned long long ne) {
+    EX_CHECK_ARG(e && e->slots_ok && (s == 0 || s == 1), "no such slot");
+    EX_CHECK_ARG(k >= 0 && k <= e->max_chunk_verts && ne <= e->max_chunk_edges, "gather larger than the slots");
+    EX_CUDA(cudaSetDevice(e->dev));
+    Slot& sl = e->slot[s];
+    if (!e->zc) {
+        EX_CUDA(cudaMemcpyAsync(sl.d_vids, sl.h_vids, (size_t)k * sizeof(int), cudaMemcpyHostToDevice, sl.st));
+        EX_CUDA(cudaMemcpyAsync(sl.d_off, sl.h_off, ((size_t)k + 1) * sizeof(ull), cudaMemcpyHostToDevice, sl.st));
+        if (ne) EX_CUDA(cudaMemcpyAsync(sl.d_edges, sl.h_edges, ne * sizeof(int), cudaMemcpyHostToDevice, sl.st));
+    }
+    if (k) {
+        PushArgs a = push_args(e, 1 + s);
+        a.vids = sl.d_vids; a.off = sl.d_off; a.gedges = sl.d_edges; a.gk = (unsigned)k;
+        EX_CUDA(cudaMemsetAsync(e->d_hubcnt + 1 + s, 0, sizeof(ull), sl.st));
+        launch_push<SRC_GATHER>(e, a, grid_for(e, (ull)k), sl.st);
+        EX_CUDA(cudaGetLastError());
+    }
+    EX_CUDA(cudaEventRecord(sl.done, sl.st));
+    sl.busy = true;
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_hot_setup(excent_engine* e, int nh, const int32_t* ids, const unsigned long long* off,
+                                       const uint32_t* hot_bitmap) {
+    EX_CHECK_ARG(e && nh >= 1 && ids && off && hot_bitmap, "bad argument");
+    EX_CUDA(cudaSetDevice(e->dev));
+    EX_CHECK_ARG(!e->d_hedges, "hot cache already set up");
+    invalidate_graph(e);
+    const size_t words = ((size_t)e->n + 31) / 32;
+    const ull he = off[nh];
+    bool ok = cudaMalloc((void**)&e->d_hedges, std::max<ull>(he, 1) * sizeof(int)) == cudaSuccess;
+    ok = ok && cudaMalloc((void**)&e->d_hids, (size_t)nh * sizeof(int)) == cudaSuccess;
+    ok = ok && cudaMalloc((void**)&e->d_hoff, ((size_t)nh + 1) * sizeof(ull)) == cudaSuccess;
+    ok = ok && cudaMalloc((void**)&e->d_hot, words * sizeof(uint32_t)) == cudaSuccess;
+    ok = ok && cudaMalloc((void**)&e->d_hlist, (size_t)nh * sizeof(int)) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        void* ps[] = {e->d_hedges, e->d_hids, e->d_hoff, e->d_hot, e->d_hlist};
+        for (void* p : ps) if (p) cudaFree(p);
+        e->d_hedges = nullptr; e->d_hids = nullptr; e->d_hoff = nullptr; e->d_hot = nullptr; e->d_hlist = nullptr;
+        e->nh = 0;
+        EX_FAIL(EXCENT_ERR_NOMEM, "degree cache: could not allocate %d lists (%.2f GB)", nh, he * 4.0 / 1e9);
+    }
+    EX_CUDA(cudaMemcpy(e->d_hids, ids, (size_t)nh * sizeof(int), cudaMemcpyHostToDevice));
+    EX_CUDA(cudaMemcpy(e->d_hoff, off, ((size_t)nh + 1) * sizeof(ull), cudaMemcpyHostToDevice));
+    EX_CUDA(cudaMemcpy(e->d_hot, hot_bitmap, words * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    e->nh = nh;
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_push_hot(excent_engine* e, int lo, int hi, int after_slots) {
+    EX_CHECK_ARG(e && e->d_hedges, "no hot cache");
+    EX_CHECK_ARG(lo >= 0 && lo <= hi && hi <= e->nh, "bad hot range");
+    EX_CUDA(cudaSetDevice(e->dev));
+    if (after_slots && e->slots_ok)
+        for (Slot& s : e->slot) if (s.busy) EX_CUDA(cudaStreamWaitEvent(e->s_main, s.done, 0));
+    if (hi == lo) return EXCENT_OK;
+    EX_CUDA(cudaMemsetAsync(&e->d_ctrl->hcount, 0, sizeof(unsigned), e->s_main));
+    const int grid = (int)std::min<long long>(((long long)(hi - lo) + BLOCK - 1) / BLOCK, (long long)e->sms * 8);
+    if (e->L == 1) k_compact_hot<1><<<grid, BLOCK, 0, e->s_main>>>(lo, hi, e->d_hids, e->d_r, e->M, e->d_hlist, e->d_ctrl);
+    else k_compact_hot<4><<<grid, BLOCK, 0, e->s_main>>>(lo, hi, e->d_hids, e->d_r, e->M, e->d_hlist, e->d_ctrl);
+    e->launches++;
+    EX_CUDA(cudaMemsetAsync(e->d_hubcnt, 0, sizeof(ull), e->s_main));
+    PushArgs a = push_args(e, 0);
+    launch_push<SRC_HOT>(e, a, grid_for(e, (ull)(hi - lo)), e->s_main);
+    EX_CUDA(cudaGetLastError());
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_sync(excent_engine* e) {
+    EX_CHECK_ARG(e, "null engine");
+    EX_CUDA(cudaSetDevice(e->dev));
+    EX_CUDA(cudaStreamSynchronize(e->s_main));
+    if (e->slots_ok) for (Slot& s : e->slot) { EX_CUDA(cudaStreamSynchronize(s.st)); s.busy = false; }
+    int err = 0;
+    EX_CUDA(cudaMemcpy(&err, &e->d_ctrl->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) EX_FAIL(EXCENT_ERR_STATE, "device capacity check failed (hub queue overflow)");
+    return EXCENT_OK;
+}
+
+// One pass of the device solve: snapshot -> plan -> push -> hubs. With ev,
+// events are recorded between the kernels.
+static void enqueue_pass(excent_engine* e, double list_frac, int max_passes, cudaGraphConditionalHandle cond,
+                         int use_cond, cudaStream_t st, cudaEvent_t* ev = nullptr) {
+    if (ev) cudaEventRecord(ev[0], st);
+    launch_snapshot(e, false, st);
+    if (ev) cudaEventRecord(ev[1], st);
+    k_plan<<<1, 1024, 0, st>>>(e->nc, e->d_cv0, e->n, e->d_cnt, e->d_cmode, list_frac, max_passes, e->d_wt_type,
+                               e->d_wt_prefix, e->d_ctrl, e->d_hubcnt, e->d_log, e->log_cap, cond, use_cond);
+    e->launches++;
+    if (ev) cudaEventRecord(ev[2], st);
+    PushArgs a = push_args(e, 0);
+    if (!ev) {
+        launch_push<SRC_TABLE>(e, a, e->grid_push, st);
+        return;
+    }
+    if (e->L == 1) k_push<1, SRC_TABLE><<<e->grid_push, BLOCK, 0, st>>>(a);
+    else k_push<4, SRC_TABLE><<<e->grid_push, BLOCK, 0, st>>>(a);
+    cudaEventRecord(ev[3], st);
+    if (e->L == 1) k_hub<1><<<e->grid_push, BLOCK, 0, st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap);
+    else k_hub<4><<<e->grid_push, BLOCK, 0, st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap);
+    cudaEventRecord(ev[4], st);
+    e->launches += 2;
+}
+
+static int build_graph(excent_engine* e, double list_frac, int max_passes) {
+    if (e->gexec && e->graph_max_passes == max_passes && e->graph_list_frac == list_frac) return EXCENT_OK;
+    invalidate_graph(e);
+    cudaGraph_t g;
+    EX_CUDA(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle h;
+    EX_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    EX_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    // capture one pass into the body graph
+    cudaStream_t cs;
+    EX_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    EX_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    const ull before = e->launches;
+    enqueue_pass(e, list_frac, max_passes, h, 1, cs);
+    e->launches = before;
+    cudaGraph_t captured;
+    cudaError_t ce = cudaStreamEndCapture(cs, &captured);
+    cudaStreamDestroy(cs);
+    EX_CUDA(ce);
+    EX_CUDA(cudaGraphInstantiate(&e->gexec, g, 0));
+    e->graph = g;
+    e->graph_max_passes = max_passes;
+    e->graph_list_frac = list_frac;
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_solve(excent_engine* e, double list_frac, int max_passes, int use_graph) {
+    EX_CHECK_ARG(e, "null engine");
+    EX_CHECK_ARG(max_passes >= 0 && max_passes < e->log_cap, "max_passes must be < %d", e->log_cap);
+    for (int c = 0; c < e->nc; c++)
+        EX_CHECK_ARG(e->loaded[c], "chunk %d is not loaded in the edge cache (device solve needs every chunk cached)", c);
+    EX_CUDA(cudaSetDevice(e->dev));
+    std::vector<uint8_t> cm(e->nc, 1);
+    EX_CUDA(cudaMemcpyAsync(e->d_cmode, cm.data(), e->nc, cudaMemcpyHostToDevice, e->s_main));
+    EX_TRY(init_state(e));
+    if (use_graph) {
+        EX_TRY(build_graph(e, list_frac, max_passes));
+        EX_CUDA(cudaGraphLaunch(e->gexec, e->s_main));
+        EX_CUDA(cudaStreamSynchronize(e->s_main));
+        EX_CUDA(cudaMemcpy(e->h_ctrl, e->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+        e->launches += 4ull * (e->h_ctrl->pass + 1);
+    } else {
+        for (int p = 0; p <= max_passes; p++) {
+            enqueue_pass(e, list_frac, max_passes, 0, 0, e->s_main, e->prof ? e->ev : nullptr);
+            EX_CUDA(cudaGetLastError());
+            EX_CUDA(cudaMemcpyAsync(e->h_ctrl, e->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, e->s_main));
+            EX_CUDA(cudaStreamSynchronize(e->s_main));
+            if (e->prof && !e->h_ctrl->done) {
+                for (int k = 0; k < 4; k++) {
+                    float ms = 0;
+                    EX_CUDA(cudaEventElapsedTime(&ms, e->ev[k], e->ev[k + 1]));
+                    e->prof_ms[k] += ms;
+                }
+                e->prof_passes++;
+            }
+            if (e->h_ctrl->done) break;
+        }
+    }
+    EX_CUDA(cudaGetLastError());
+    if (e->h_ctrl->err) EX_FAIL(EXCENT_ERR_STATE, "device capacity check failed (hub queue overflow)");
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_stats(excent_engine* e, excent_stats* st, excent_pass_log* log, int cap) {
+    EX_CHECK_ARG(e, "null engine");
+    EX_CUDA(cudaSetDevice(e->dev));
+    EX_CUDA(cudaDeviceSynchronize());
+    Ctrl c;
+    EX_CUDA(cudaMemcpy(&c, e->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+    const int np = std::min(c.pass, e->log_cap);
+    std::vector<PassRec> recs(np);
+    if (np) EX_CUDA(cudaMemcpy(recs.data(), e->d_log, np * sizeof(PassRec), cudaMemcpyDeviceToHost));
+    if (st) {
+        memset(st, 0, sizeof(*st));
+        st->passes = c.pass;
+        st->pushed = c.pushed;
+        ull nl = 0, nr = 0;
+        for (auto& r : recs) { nl += r.n_list; nr += r.n_range; }
+        st->n_list = nl + e->n_list;
+        st->n_range = nr + e->n_range;
+        for (int k = 0; k < MAXM; k++) st->rsum[k] = c.rsum[k];
+    }
+    if (log) {
+        for (int p = 0; p < np && p < cap; p++) {
+            excent_pass_log& L = log[p];
+            L.pending = recs[p].pending; L.demand = recs[p].demand; L.hot_pending = recs[p].hot_pending;
+            L.pushed = (p + 1 < np ? recs[p + 1].pushed_before : c.pushed) - recs[p].pushed_before;
+            for (int k = 0; k < MAXM; k++) L.rsum[k] = recs[p].rsum[k];
+            L.n_list = recs[p].n_list; L.n_range = recs[p].n_range;
+        }
+    }
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_read(excent_engine* e, int i, int residual, float* out, unsigned long long v0,
+                                  unsigned long long count) {
+    EX_CHECK_ARG(e && out && i >= 0 && i < e->nm && v0 + count <= (ull)e->n, "bad argument");
+    EX_CUDA(cudaSetDevice(e->dev));
+    EX_CUDA(cudaDeviceSynchronize());
+    const void* src = residual ? e->d_r : e->d_x;
+    if (e->L == 1) {
+        EX_CUDA(cudaMemcpy(out, (const float*)src + v0, count * sizeof(float), cudaMemcpyDeviceToHost));
+    } else {
+        k_extract<<<e->sms * 8, BLOCK, 0, e->s_main>>>(e->n, (const float4*)src, i, e->d_tmp);
+        e->launches++;
+        EX_CUDA(cudaGetLastError());
+        EX_CUDA(cudaMemcpyAsync(out, e->d_tmp + v0, count * sizeof(float), cudaMemcpyDeviceToHost, e->s_main));
+        EX_CUDA(cudaStreamSynchronize(e->s_main));
+    }
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_write(excent_engine* e, int i, const float* x, const float* r) {
+    EX_CHECK_ARG(e && i >= 0 && i < e->nm, "bad argument");
+    EX_CUDA(cudaSetDevice(e->dev));
+    EX_CUDA(cudaDeviceSynchronize());
+    const float* srcs[2] = {x, r};
+    void* dsts[2] = {e->d_x, e->d_r};
+    for (int j = 0; j < 2; j++) {
+        if (!srcs[j]) continue;
+        if (e->L == 1) EX_CUDA(cudaMemcpy(dsts[j], srcs[j], (size_t)e->n * sizeof(float), cudaMemcpyHostToDevice));
+        else {
+            EX_CUDA(cudaMemcpy(e->d_tmp, srcs[j], (size_t)e->n * sizeof(float), cudaMemcpyHostToDevice));
+            k_insert<<<e->sms * 8, BLOCK>>>(e->n, (float4*)dsts[j], i, e->d_tmp);
+            e->launches++;
+            EX_CUDA(cudaGetLastError());
+            EX_CUDA(cudaDeviceSynchronize());
+        }
+    }
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_stream(excent_engine* e, void** stream) {
+    EX_CHECK_ARG(e && stream, "null argument");
+    *stream = (void*)e->s_main;
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_profile(excent_engine* e, int enable) {
+    EX_CHECK_ARG(e, "null engine");
+    EX_CUDA(cudaSetDevice(e->dev));
+    if (enable && !e->ev[0])
+        for (cudaEvent_t& ev : e->ev) EX_CUDA(cudaEventCreate(&ev));
+    e->prof = enable != 0;
+    for (double& t : e->prof_ms) t = 0;
+    e->prof_passes = 0;
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_profile_read(excent_engine* e, double* ms, unsigned long long* passes) {
+    EX_CHECK_ARG(e && ms, "null argument");
+    for (int k = 0; k < 4; k++) ms[k] = e->prof_ms[k];
+    if (passes) *passes = e->prof_passes;
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_launches(excent_engine* e, unsigned long long* launches) {
+    EX_CHECK_ARG(e && launches, "null argument");
+    *launches = e->launches;
+    return EXCENT_OK;
+}

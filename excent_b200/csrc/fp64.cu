@@ -1,0 +1,194 @@
+// fp64.cu -- the FP64 steps that run on the device: the eigenvector lambda1 /
+// normalisation power iteration and the Katz fixed-point mean that give a
+// graph's "given constants" (the reference computes them in
+// tools/excent_params.cu:133-172), and an FP64 Jacobi / power-iteration
+// solve of PageRank, Katz and eigenvector centrality for verification of
+// large graphs (tools/centrality_reference.cu:31-59, 184-214).
+//
+// Graphs are device-resident CSR (offsets u64[n+1], lists i32[m]) and
+// symmetric, so a pull over out-lists equals the in-neighbour sum.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+#include "common.h"
+#include "device.cuh"
+
+namespace excent {
+
+// y[v] = c + s * sum_{u in N(v)} x[u] (/ L(u) if divdeg); one warp per vertex.
+// If mx is given: mx[0] = max |y - x|, mx[1] = max |y| (as ordered bit patterns).
+__global__ void k_pull64(int n, const ull* idx, const int* adj, const double* x, double* y, double c, double s,
+                         int divdeg, ull* mx) {
+    const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= n) return;
+    double acc = 0;
+    for (ull e = idx[w] + lane; e < idx[w + 1]; e += 32) {
+        const int u = adj[e];
+        acc += divdeg ? x[u] / (double)(idx[u + 1] - idx[u]) : x[u];
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) {
+        const double nv = c + s * acc;
+        y[w] = nv;
+        if (mx) {
+            atomicMax(&mx[0], (ull)__double_as_longlong(fabs(nv - x[w])));
+            atomicMax(&mx[1], (ull)__double_as_longlong(fabs(nv)));
+        }
+    }
+}
+
+// out[0] += sum x^2, out[1] += sum x, out[2] = max |x - y| (bit pattern) if y
+__global__ void k_norms64(int n, const double* x, const double* y, double* out, ull* mx) {
+    double a = 0, b = 0, d = 0;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
+        a += x[v] * x[v];
+        b += x[v];
+        if (y) d = fmax(d, fabs(x[v] - y[v]));
+    }
+    a = warp_sum(a);
+    b = warp_sum(b);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d = fmax(d, __shfl_down_sync(FULL, d, o));
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&out[0], a);
+        atomicAdd(&out[1], b);
+        if (y) atomicMax(mx, (ull)__double_as_longlong(d));
+    }
+}
+
+__global__ void k_scale64(int n, double* x, double f, double add) {
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x)
+        x[v] = x[v] * f + add;
+}
+
+}  // namespace excent
+
+using namespace excent;
+
+namespace {
+struct Bufs {
+    double* v[2] = {nullptr, nullptr};
+    double* red = nullptr;
+    ull* mx = nullptr;
+    ~Bufs() {
+        for (double* p : v) if (p) cudaFree(p);
+        if (red) cudaFree(red);
+        if (mx) cudaFree(mx);
+    }
+};
+
+int norms(int n, const double* x, const double* y, Bufs& B, int grid, double* ss, double* sum, double* maxdiff) {
+    EX_CUDA(cudaMemset(B.red, 0, 2 * sizeof(double)));
+    EX_CUDA(cudaMemset(B.mx, 0, sizeof(ull)));
+    k_norms64<<<grid, 256>>>(n, x, y, B.red, B.mx);
+    double h[2];
+    ull m = 0;
+    EX_CUDA(cudaMemcpy(h, B.red, sizeof h, cudaMemcpyDeviceToHost));
+    EX_CUDA(cudaMemcpy(&m, B.mx, sizeof m, cudaMemcpyDeviceToHost));
+    if (ss) *ss = h[0];
+    if (sum) *sum = h[1];
+    if (maxdiff) { double d; memcpy(&d, &m, 8); *maxdiff = d; }
+    return EXCENT_OK;
+}
+}  // namespace
+
+extern "C" int excent_params_fp64(int device, int n, const unsigned long long* d_idx, const int32_t* d_adj,
+                                  double katz_numerator, double* out) {
+    EX_CHECK_ARG(n >= 1 && d_idx && d_adj && out, "bad argument");
+    EX_CUDA(cudaSetDevice(device));
+    int sms = 0;
+    EX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const int G = sms * 8;
+    const unsigned wb = (unsigned)(((long long)n * 32 + 255) / 256);
+    Bufs B;
+    for (auto& p : B.v) if (cudaMalloc(&p, (size_t)n * sizeof(double)) != cudaSuccess) { cudaGetLastError(); EX_FAIL(EXCENT_ERR_NOMEM, "params: vectors do not fit"); }
+    EX_CUDA(cudaMalloc(&B.red, 2 * sizeof(double)));
+    EX_CUDA(cudaMalloc(&B.mx, sizeof(ull)));
+    // lambda1: unit all-ones start, y = A x, lam = ||y||, x = y / lam; stop when
+    // |lam - lamPrev| / lam < 1e-12 after 10 sweeps (tools/excent_params.cu:133-147)
+    k_scale64<<<G, 256>>>(n, B.v[0], 0.0, 1.0 / std::sqrt((double)n));
+    double lam = 0, lamPrev = 0, ss = 0, vsum = 0;
+    int pit = 0;
+    for (; pit < 5000; pit++) {
+        k_pull64<<<wb, 256>>>(n, d_idx, d_adj, B.v[0], B.v[1], 0.0, 1.0, 0, nullptr);
+        EX_TRY(norms(n, B.v[1], nullptr, B, G, &ss, nullptr, nullptr));
+        lam = std::sqrt(ss);
+        k_scale64<<<G, 256>>>(n, B.v[1], 1.0 / lam, 0.0);
+        std::swap(B.v[0], B.v[1]);
+        if (pit > 10 && std::fabs(lam - lamPrev) / lam < 1e-12) break;
+        lamPrev = lam;
+    }
+    EX_TRY(norms(n, B.v[0], nullptr, B, G, nullptr, &vsum, nullptr));
+    const double meanEV = vsum * vsum / n;
+    // Katz fixed point x = 1 + alpha A x, alpha = katz_numerator / lambda1, for its mean (:150-162)
+    const double alpha = katz_numerator / lam;
+    k_scale64<<<G, 256>>>(n, B.v[0], 0.0, 1.0);
+    double meanK = 0;
+    for (int it = 0; it < 5000; it++) {
+        k_pull64<<<wb, 256>>>(n, d_idx, d_adj, B.v[0], B.v[1], 1.0, alpha, 0, nullptr);
+        std::swap(B.v[0], B.v[1]);
+        double sum = 0;
+        EX_TRY(norms(n, B.v[0], nullptr, B, G, nullptr, &sum, nullptr));
+        const double nm = sum / n;
+        if (std::fabs(nm - meanK) / nm < 1e-12) { meanK = nm; break; }
+        meanK = nm;
+    }
+    EX_CUDA(cudaDeviceSynchronize());
+    out[0] = lam; out[1] = alpha; out[2] = meanEV; out[3] = meanK; out[4] = pit;
+    return EXCENT_OK;
+}
+
+extern "C" int excent_reference_fp64(int device, int n, const unsigned long long* d_idx, const int32_t* d_adj,
+                                     int kind, double alpha, double beta, double tol, int maxit, double* x_out,
+                                     int* iterations) {
+    EX_CHECK_ARG(n >= 1 && d_idx && d_adj && x_out && kind >= 0 && kind <= 2, "bad argument");
+    EX_CUDA(cudaSetDevice(device));
+    int sms = 0;
+    EX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const int G = sms * 8;
+    const unsigned wb = (unsigned)(((long long)n * 32 + 255) / 256);
+    Bufs B;
+    for (auto& p : B.v) if (cudaMalloc(&p, (size_t)n * sizeof(double)) != cudaSuccess) { cudaGetLastError(); EX_FAIL(EXCENT_ERR_NOMEM, "reference: vectors do not fit"); }
+    EX_CUDA(cudaMalloc(&B.red, 2 * sizeof(double)));
+    EX_CUDA(cudaMalloc(&B.mx, 2 * sizeof(ull)));
+    double c = 0, s = 1;
+    int divdeg = 0;
+    if (kind == 0) { c = 0.15; s = 0.85; divdeg = 1; }
+    else if (kind == 1) { c = beta; s = alpha; }
+    k_scale64<<<G, 256>>>(n, B.v[0], 0.0, kind == 0 ? 0.15 : 1.0);
+    int it = 0;
+    double rel = 1;
+    for (; it < maxit && rel > tol; it++) {
+        if (kind == 2) {
+            k_pull64<<<wb, 256>>>(n, d_idx, d_adj, B.v[0], B.v[1], 0.0, 1.0, 0, nullptr);
+            double ss = 0;
+            EX_TRY(norms(n, B.v[1], nullptr, B, G, &ss, nullptr, nullptr));
+            k_scale64<<<G, 256>>>(n, B.v[1], 1.0 / std::sqrt(ss), 0.0);
+            double md = 0;
+            EX_TRY(norms(n, B.v[1], B.v[0], B, G, nullptr, nullptr, &md));
+            rel = it == 0 ? 1.0 : md;
+        } else {
+            EX_CUDA(cudaMemset(B.mx, 0, 2 * sizeof(ull)));
+            k_pull64<<<wb, 256>>>(n, d_idx, d_adj, B.v[0], B.v[1], c, s, divdeg, B.mx);
+            ull h[2];
+            EX_CUDA(cudaMemcpy(h, B.mx, sizeof h, cudaMemcpyDeviceToHost));
+            double d, m;
+            memcpy(&d, &h[0], 8);
+            memcpy(&m, &h[1], 8);
+            rel = d / m;
+        }
+        std::swap(B.v[0], B.v[1]);
+    }
+    EX_CUDA(cudaMemcpy(x_out, B.v[0], (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (kind == 2) {  // unit L2 norm, sign fixed by the sum (tools/centrality_reference.cu:71-76)
+        double s2 = 0, t = 0;
+        for (int i = 0; i < n; i++) { s2 += x_out[i] * x_out[i]; t += x_out[i]; }
+        const double f = (t < 0 ? -1.0 : 1.0) / std::sqrt(s2);
+        for (int i = 0; i < n; i++) x_out[i] *= f;
+    }
+    if (iterations) *iterations = it;
+    return EXCENT_OK;
+}

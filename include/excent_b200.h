@@ -1,0 +1,252 @@
+/*
+ * excent_b200.h -- C ABI of libexcent_b200.so, the B200 (sm_100a) engine for
+ * ExCent's asynchronous delta-push centrality path (PageRank, Katz,
+ * eigenvector, and the single-stream `all` pass).
+ *
+ * Plain C types only: pointers, sizes, status codes. Every call returns an
+ * EXCENT_* status; on failure excent_last_error() holds a message (thread
+ * local). Nothing here exits the process.
+ *
+ * The reference (SPADE-IITJ/ExCent) is a monolithic CLI whose kernels are
+ * launched directly from main(); its internal seam is the Measures table
+ * passed by value to every kernel (src/excent.cu:29-37) and the launches at
+ * src/excent.cu:663 (snapshot), :642-649 (compact + push of a chunk in GPU
+ * memory), :738 (push of a gathered list), :618-624 (hot cache) and :705 (hot
+ * fill). Each entry point below names the reference code it replaces.
+ * Reference paths are relative to the reference project.
+ */
+#ifndef EXCENT_B200_H
+#define EXCENT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+#define EXCENT_OK 0
+#define EXCENT_ERR_ARG 1     /* bad argument (message says which) */
+#define EXCENT_ERR_CUDA 2    /* a CUDA runtime call failed */
+#define EXCENT_ERR_IO 3      /* open / read / short read / bad file */
+#define EXCENT_ERR_NOMEM 4   /* a device or pinned allocation failed */
+#define EXCENT_ERR_STATE 5   /* call out of order (e.g. no graph uploaded) */
+#define EXCENT_ERR_TIMEOUT 6 /* a bounded device wait gave up */
+
+/* measure kinds, as src/excent.cu:22 numbers them */
+#define EXCENT_PR 0
+#define EXCENT_KATZ 1
+#define EXCENT_EV 2
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* excent_last_error(void);
+/* Library ABI version (major * 100 + minor). */
+int excent_version(void);
+
+/* ------------------------------------------------------------ measures */
+
+/* The per-run measure table: replaces struct Measures (src/excent.cu:29-37)
+ * together with the init constants of k_init (:41-47). Vectors are per
+ * measure, in run order. */
+typedef struct excent_measures {
+    int nm;            /* number of measures, 1..3 */
+    int kind[3];       /* EXCENT_PR / EXCENT_KATZ / EXCENT_EV */
+    float eps[3];      /* pending iff |r| > eps */
+    float scale[3];    /* push weight numerator: d, alpha, or 1/lambda */
+    int divdeg[3];     /* 1: weight = scale / deg(v) (PageRank) */
+    double beta;       /* Katz initial residual */
+    double lambda;     /* eigenvector initial residual deg/lambda - 1 */
+} excent_measures;
+
+/* Build the table for --measure pr|katz|ev|all with the reference's
+ * validation and float rounding (src/excent.cu:307-316, 344-351). Negative
+ * alpha / lambda / eps mean "not given". */
+int excent_measures_make(excent_measures* out, const char* measure, double alpha, double beta, double lambda,
+                         double eps_pr, double eps_katz, double eps_ev);
+
+/* ------------------------------------------------------------ device engine */
+
+typedef struct excent_engine excent_engine;
+
+/* Create an engine on `device` for a graph of n vertices and m edges split
+ * into nc chunks whose first vertices are chunk_v0[0..nc) and edge bounds
+ * chunk_e[0..nc] (host arrays). Allocates the per-vertex state (values,
+ * residuals, offsets, bitmap, pending lists, demand table). Replaces the
+ * allocations of src/excent.cu:335-369. */
+int excent_engine_create(int device, int n, unsigned long long m, const excent_measures* measures, int nc,
+                         const int* chunk_v0, const unsigned long long* chunk_e, excent_engine** out);
+int excent_engine_destroy(excent_engine* e);
+
+/* Copy offsets idx[v0 .. v0+count) from host memory (pageable or pinned);
+ * replaces the upload loop of src/excent.cu:360-369. */
+int excent_engine_upload_offsets(excent_engine* e, const unsigned long long* idx, unsigned long long v0,
+                                 unsigned long long count);
+
+/* Copy a whole graph that is already in device memory (idx[n+1], adj[m]
+ * device pointers, e.g. from excent_rmat_generate) into the engine: offsets
+ * and a full edge cache, every chunk marked loaded. */
+int excent_engine_upload_device(excent_engine* e, const unsigned long long* d_idx, const int32_t* d_adj);
+
+/* Reserve the HBM edge cache for the first `edges` edges of the graph (the
+ * resident chunk prefix); replaces the per-chunk cudaMalloc loop of
+ * src/excent.cu:410-421. Returns EXCENT_ERR_NOMEM (and leaves no cache) if the
+ * allocation fails. */
+int excent_engine_reserve_cache(excent_engine* e, unsigned long long edges);
+/* Copy edges [e0, e1) from host memory into the edge cache and mark the
+ * chunks fully inside it as loaded. */
+int excent_engine_load_cache(excent_engine* e, unsigned long long e0, unsigned long long e1, const int32_t* edges);
+/* Mark chunk c as loaded (its edges were copied by a streamed push with
+ * cache fill); src/excent.cu:707. */
+int excent_engine_set_loaded(excent_engine* e, int c, int loaded);
+
+/* k_init for every measure (src/excent.cu:370-372) and reset of the pass state. */
+int excent_engine_init(excent_engine* e);
+
+/* One demand snapshot (src/excent.cu:660-665): zero the demand table, launch
+ * the snapshot kernel and copy back cnt[2*nc] (interleaved pending count and
+ * pending degree sum per chunk), the hot pending count and the FP64 sum of
+ * |r| per measure. use_hot: skip cached high-degree vertices (pass > 0 in hot
+ * mode, src/excent.cu:662). Any output pointer may be NULL. */
+int excent_engine_snapshot(excent_engine* e, int use_hot, unsigned long long* cnt, unsigned long long* hotpend,
+                           double* rsum);
+/* Copy the pending bitmap (ceil(n/32) words) to the host (src/excent.cu:678). */
+int excent_engine_bitmap(excent_engine* e, uint32_t* words);
+/* Copy the snapshot's pending list of chunk c (unordered) and its length. */
+int excent_engine_chunk_list(excent_engine* e, int c, int32_t* ids, unsigned int* k);
+
+/* Push every chunk whose mode[c] == 1 from the HBM edge cache in one launch,
+ * each as its pending list when cnt < list_frac * chunk vertices, else as
+ * its whole vertex range with the push-time re-check. Replaces the resident
+ * loop and launch_chunk (src/excent.cu:629-652, 684-688). mode and cnt are
+ * host arrays (cnt as returned by the last snapshot). */
+int excent_engine_push_cached(excent_engine* e, const unsigned char* mode, const unsigned long long* cnt,
+                              double list_frac);
+
+/* Pinned double-buffered staging (src/excent.cu:224-233, 374-390). Two slots,
+ * each with host buffers for edges (max_chunk_edges), vertex ids and offsets
+ * (max_chunk_verts), device mirrors, a stream and an event. zero_copy maps
+ * the host buffers into the device address space instead (:376-379). */
+int excent_engine_slots_create(excent_engine* e, unsigned long long max_chunk_edges, int max_chunk_verts,
+                               int zero_copy);
+/* Host pointers of slot s (0 or 1) for the planner to fill. */
+int excent_engine_slot_buffers(excent_engine* e, int s, int32_t** edges, int32_t** vids, unsigned long long** off);
+/* Wait until slot s's previous work finished (src/excent.cu:599-601). */
+int excent_engine_slot_wait(excent_engine* e, int s);
+/* Streamed chunk c staged in slot s: copy its edges to the device (into the
+ * edge cache when cache_fill and the chunk is resident), optionally fill the
+ * hot cache lists of hot ids [hlo, hhi) from it (k_fill_hot, :704-705), then
+ * push it as list or range (launch_chunk). Asynchronous on the slot stream.
+ * src/excent.cu:696-707. */
+int excent_engine_push_stream(excent_engine* e, int s, int c, const unsigned long long* cnt, double list_frac,
+                              int cache_fill, int hlo, int hhi);
+/* Gathered lists in slot s: k vertex ids, k+1 offsets, ne edges; copy and
+ * push (src/excent.cu:732-739). Asynchronous on the slot stream. */
+int excent_engine_push_gather(excent_engine* e, int s, int k, unsigned long long ne);
+
+/* Degree (hot) cache of nh high-degree vertices: ids ascending, list offsets
+ * off[nh+1], and the hot bitmap (ceil(n/32) words). Returns EXCENT_ERR_NOMEM
+ * and leaves no cache when it does not fit (src/excent.cu:492-503). */
+int excent_engine_hot_setup(excent_engine* e, int nh, const int32_t* ids, const unsigned long long* off,
+                            const uint32_t* hot_bitmap);
+/* Push the pending hot vertices among hot ids [lo, hi) from the hot cache,
+ * after the slots' outstanding work (src/excent.cu:615-628, 745-748). The
+ * pending count stays on the device: no host synchronisation per range. */
+int excent_engine_push_hot(excent_engine* e, int lo, int hi, int after_slots);
+
+/* Wait for all engine streams. */
+int excent_engine_sync(excent_engine* e);
+
+/* Device solve of a fully cached graph (every chunk resident and loaded):
+ * init, then passes of snapshot -> on-device fetch plan -> push until no
+ * vertex is pending or max_passes, with no host round trip per pass. With
+ * use_graph the pass is one CUDA graph with a conditional while node.
+ * Per-pass log and totals are kept for excent_engine_stats. */
+int excent_engine_solve(excent_engine* e, double list_frac, int max_passes, int use_graph);
+
+typedef struct excent_pass_log {
+    unsigned long long pending;   /* pending vertices at the snapshot */
+    unsigned long long demand;    /* their total degree */
+    unsigned long long hot_pending;
+    unsigned long long pushed;    /* adjacency entries pushed in the pass */
+    double rsum[3];               /* FP64 sum of |r| per measure at the snapshot */
+    int n_list, n_range;          /* chunks pushed as lists / whole ranges */
+} excent_pass_log;
+
+typedef struct excent_stats {
+    int passes;                   /* passes that pushed (the reference's "passes") */
+    unsigned long long pushed;    /* adjacency entries pushed in total */
+    unsigned long long n_list, n_range;
+    double rsum[3];               /* final FP64 sum of |r| per measure */
+} excent_stats;
+
+/* Totals of the last solve, and up to cap pass records. */
+int excent_engine_stats(excent_engine* e, excent_stats* st, excent_pass_log* log, int cap);
+
+/* Copy values x (or residuals r) of measure i (run order) for vertices
+ * [v0, v0+count) to the host as float32 (src/excent.cu:763-777). */
+int excent_engine_read(excent_engine* e, int i, int residual, float* out, unsigned long long v0,
+                       unsigned long long count);
+/* Overwrite values and residuals of measure i from host float32 arrays of n
+ * entries (either may be NULL to keep it). Test hook. */
+int excent_engine_write(excent_engine* e, int i, const float* x, const float* r);
+
+/* --trace-pending: a uint16 counter per vertex of the passes in which it was
+ * pending (src/excent.cu:76, 606-607, 779-789). enable before init. */
+int excent_engine_trace(excent_engine* e, int enable);
+int excent_engine_read_trace(excent_engine* e, uint16_t* out);
+
+/* The engine's main CUDA stream (cudaStream_t), for callers that time
+ * its work with their own events. */
+int excent_engine_stream(excent_engine* e, void** stream);
+/* Per-kernel timing of the device solve run without a graph (use_graph=0):
+ * events around the snapshot, plan, push and hub kernels of every pushing
+ * pass. profile_read returns the summed milliseconds {snapshot, plan, push,
+ * hub} and the pass count since profiling was enabled. */
+int excent_engine_profile(excent_engine* e, int enable);
+int excent_engine_profile_read(excent_engine* e, double* ms, unsigned long long* passes);
+
+/* Number of device kernel launches this engine issued so far. */
+int excent_engine_launches(excent_engine* e, unsigned long long* launches);
+
+/* ------------------------------------------------------------ FP64 tools */
+
+/* Given constants of a symmetric device-resident graph (offsets and lists
+ * are device pointers): lambda1 by FP64 power iteration from the unit
+ * all-ones vector (stop when the relative change of lambda1 < 1e-12 after 10
+ * sweeps, <= 5000), the eigenvector fixed-point mean (v1 . 1)^2 / n, Katz
+ * alpha = katz_numerator / lambda1 and the mean of x = 1 + alpha A x.
+ * out = {lambda1, alpha, meanEV, meanKatz, sweeps}. tools/excent_params.cu:133-163. */
+int excent_params_fp64(int device, int n, const unsigned long long* d_idx, const int32_t* d_adj,
+                       double katz_numerator, double* out);
+/* FP64 reference solution on the device: kind 0 PageRank (x0 = 0.15,
+ * x = 0.15 + 0.85 sum x_u / L(u)), 1 Katz (x = beta + alpha sum x_u),
+ * 2 eigenvector (power iteration, unit L2 norm, sign fixed by the sum); Jacobi
+ * until max|dx| / max|x| <= tol (eigenvector: max|dx| <= tol) or maxit.
+ * x_out is a host array of n doubles. tools/centrality_reference.cu:31-59, 184-214. */
+int excent_reference_fp64(int device, int n, const unsigned long long* d_idx, const int32_t* d_adj, int kind,
+                          double alpha, double beta, double tol, int maxit, double* x_out, int* iterations);
+
+/* ------------------------------------------------------------ R-MAT graphs */
+
+/* A graph held in device memory (CSR offsets, lists, optional weights). */
+typedef struct excent_dgraph excent_dgraph;
+
+/* Seeded R-MAT graph on `device`: n = 2^scale vertices, edge_factor * n / 2
+ * pairs drawn (symmetric: both directions added) or edge_factor * n
+ * (directed), quadrant probabilities a, b, c (d = 1 - a - b - c), self-loops
+ * and duplicates dropped, lists sorted. weights: also float32 weights
+ * uniform on [0.5, 1.5) per CSR edge. No reference counterpart: the
+ * reference ingests .mtx files (tools/efficient_converter.py:5-113). */
+int excent_rmat_generate(int device, int scale, int edge_factor, unsigned long long seed, double a, double b,
+                         double c, int symmetric, int weights, excent_dgraph** out);
+int excent_dgraph_info(excent_dgraph* g, int* n, unsigned long long* m);
+int excent_dgraph_device_ptrs(excent_dgraph* g, unsigned long long** idx, int32_t** adj, float** w);
+/* Copy offsets (n+1), lists (m) and weights (m, if generated) to host memory; any may be NULL. */
+int excent_dgraph_download(excent_dgraph* g, unsigned long long* idx, int32_t* adj, float* w);
+int excent_dgraph_destroy(excent_dgraph* g);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EXCENT_B200_H */

@@ -1,0 +1,91 @@
+"""Regenerate the committed golden fixtures of this directory.
+
+    python tests/golden/make_golden.py            # CPU part (needs the reference checkout)
+    python tests/golden/make_golden.py --gpu-ref [--out DIR]  # also run the reference's own CUDA tools
+
+CPU part: copies the reference's sample graph and its given constants
+(datasets/sample/sample.egr, sample.env of SPADE-IITJ/ExCent) and records
+their SHA-256. --gpu-ref (on a machine with a GPU, after `make -C oracle ref`)
+runs the reference's FP64 oracle binary (tools/centrality_reference.cu) and
+its engine binary (src/excent.cu) built from source into oracle/_ref/, and
+stores their outputs: sample_ref_<measure>.f64 (FP64 oracle vectors) and
+sample_excent_<measure>.f32 (the reference engine's result dumps).
+"""
+import hashlib
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+REF = "/root/reference/datasets/sample"
+REF_BIN = os.path.join(ROOT, "oracle", "_ref")
+
+
+def sha(p):
+    return hashlib.sha256(open(p, "rb").read()).hexdigest()
+
+
+def env_args(env, measure):
+    a = ["--measure", measure]
+    if measure in ("katz", "all"):
+        a += ["--alpha", env["ALPHA"], "--beta", env["BETA"], "--eps-katz", env["EPS_KATZ"]]
+    if measure in ("ev", "all"):
+        a += ["--lambda", env["LAMBDA"], "--eps-ev", env["EPS_EV"]]
+    if measure == "all":
+        a += ["--eps-pr", env["EPS_PR"]]
+    return a
+
+
+def read_env(p):
+    env = {}
+    for line in open(p):
+        line = line.strip()
+        if line and not line.startswith("#") and "=" in line:
+            k, v = line.split("=", 1)
+            env[k] = v
+    return env
+
+
+def main():
+    out_dir = HERE
+    if "--out" in sys.argv:
+        out_dir = sys.argv[sys.argv.index("--out") + 1]
+        os.makedirs(out_dir, exist_ok=True)
+    meta_p = os.path.join(out_dir, "golden.json")
+    meta = json.load(open(meta_p)) if os.path.exists(meta_p) else {}
+    if os.path.isdir(REF):
+        for f in ("sample.egr", "sample.env"):
+            shutil.copyfile(os.path.join(REF, f), os.path.join(HERE, f))
+        meta["sample.egr"] = sha(os.path.join(HERE, "sample.egr"))
+        meta["sample.env"] = sha(os.path.join(HERE, "sample.env"))
+    if "--gpu-ref" in sys.argv:
+        egr = os.path.join(HERE, "sample.egr")
+        env = read_env(os.path.join(HERE, "sample.env"))
+        for m in ("pr", "katz", "ev"):
+            out = os.path.join(out_dir, f"sample_ref_{m}.f64")
+            cmd = [os.path.join(REF_BIN, "centrality_reference"), egr, m, out]
+            if m == "katz":
+                cmd += ["--alpha", env["ALPHA"], "--beta", env["BETA"]]
+            r = subprocess.run(cmd, capture_output=True, text=True, check=True)
+            meta[f"centrality_reference {m}"] = r.stdout.strip()
+        tmp = os.path.join(out_dir, "_tmp_dump")
+        for m in ("pr", "katz", "ev", "all"):
+            cmd = [os.path.join(REF_BIN, "excent"), egr, *env_args(env, m), "--stream-ratio", "2",
+                   "--dump", tmp]
+            r = subprocess.run(cmd, capture_output=True, text=True, check=True,
+                               env=dict(os.environ, HOME=tempfile.mkdtemp()))
+            meta[f"excent {m}"] = [l for l in r.stdout.splitlines() if l.startswith("passes")]
+            names = ("pr", "katz", "ev") if m == "all" else (m,)
+            for k in names:
+                dst = os.path.join(out_dir, f"sample_excent_{m}_{k}.f32")
+                os.replace(f"{tmp}.{k}.bin", dst)
+    json.dump(meta, open(meta_p, "w"), indent=1, sort_keys=True)
+    print(json.dumps(meta, indent=1))
+
+
+if __name__ == "__main__":
+    main()

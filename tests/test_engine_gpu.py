@@ -1,0 +1,244 @@
+"""Parity of the CUDA engine with the oracle and with the reference's own kernels.
+
+Integer work (pending bitmap, per-chunk demand table, hot pending count,
+compacted pending lists) must be bit-exact; FP32 results are compared with the
+FP64 oracle as L1 relative error, max per-vertex error and top-k overlap.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("needs a GPU", allow_module_level=True)
+
+import excent_b200 as X  # noqa: E402
+
+
+def chunks_for(idx, cap):
+    v0, e = X.plan_chunks(idx, cap)
+    return v0, e
+
+
+def make_engine(n, idx, adj, meas, cap=None, upload_edges=True):
+    m = len(adj)
+    v0, e = chunks_for(idx, cap or max(m, 1))
+    eng = X.Engine(n, m, meas, v0, e)
+    if upload_edges:
+        eng.upload_graph(idx, adj)
+    else:
+        eng.upload_offsets(idx)
+    return eng
+
+
+def meas_for(kinds, env=None, **kw):
+    if env is not None:
+        kw = dict(alpha=float(env["ALPHA"]), lam=float(env["LAMBDA"]), eps_katz=float(env["EPS_KATZ"]),
+                  eps_ev=float(env["EPS_EV"]))
+    return X.measures(kinds, **kw)
+
+
+def bits_of(bm, n):
+    v = np.arange(n)
+    return ((bm[v >> 5] >> (v & 31)) & 1).astype(bool)
+
+
+# ------------------------------------------------------------------ reference kernels
+
+def ref_kernels():
+    p = os.path.join(O.REF_DIR, "libexcent_ref.so")
+    if not os.path.exists(p):
+        pytest.skip("reference kernel harness not built (make -C oracle ref)")
+    L = C.CDLL(p)
+    L.ref_snapshot.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.ref_compact.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.ref_init.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float, C.c_float]
+    return L
+
+
+def snapshot_case(nm, seed, n, idx, cap, hot_frac):
+    rng = np.random.default_rng(seed)
+    eps = np.array([0.01, 0.05, 0.003][:nm], dtype=np.float32)
+    r = [rng.normal(0, eps[k] * 1.2, n).astype(np.float32) for k in range(nm)]
+    # some exact-threshold values: |r| == eps is not pending
+    r[0][::97] = eps[0]
+    v0, e = chunks_for(idx, cap)
+    hot_ids = np.sort(rng.choice(n, max(1, int(hot_frac * n)), replace=False)).astype(np.int32)
+    hot = np.zeros((n + 31) // 32, dtype=np.uint32)
+    for v in hot_ids:
+        hot[v >> 5] |= np.uint32(1 << int(v & 31))
+    return eps, r, v0, e, hot_ids, hot
+
+
+@pytest.mark.parametrize("nm", [1, 2, 3])
+@pytest.mark.parametrize("cap", [37, 1000, 10 ** 9])
+@pytest.mark.parametrize("use_hot", [False, True])
+def test_snapshot_bitexact_vs_oracle_and_reference(rmat12, nm, cap, use_hot):
+    n, idx, adj = rmat12
+    eps, r, v0, e, hot_ids, hot = snapshot_case(nm, 11 + nm, n, idx, cap, 0.05)
+    kinds = ["pr", "katz", "ev"][:nm]
+    meas = X.measures("all" if nm == 3 else "pr", alpha=0.1, lam=10.0, eps_katz=1.0, eps_ev=1.0)
+    meas.nm = nm
+    for k in range(nm):
+        meas.eps[k] = float(eps[k])
+    eng = X.Engine(n, len(adj), meas, v0, e)
+    eng.upload_offsets(idx)
+    if use_hot:
+        deg = np.diff(idx.astype(np.int64))[hot_ids]
+        off = np.zeros(len(hot_ids) + 1, dtype=np.uint64)
+        off[1:] = np.cumsum(deg)
+        import excent_b200._capi as K
+        K.call("excent_engine_hot_setup", eng.h, len(hot_ids), hot_ids.ctypes.data_as(K.i32p),
+               off.ctypes.data_as(K.u64p), hot.ctypes.data_as(K.u32p))
+    eng.init()
+    eng.trace(True)
+    for k in range(nm):
+        eng.write(k, r=r[k])
+    cnt, hp, rsum = eng.snapshot(use_hot=use_hot)
+    bm = eng.bitmap()
+    tr = eng.read_trace()
+    bm_o, cnt_o, hp_o = O.snapshot(n, r, eps, idx, v0, hot if use_hot else None)
+    assert np.array_equal(bm, bm_o)
+    assert np.array_equal(cnt, cnt_o)
+    assert hp == hp_o
+    pend_any = np.zeros(n, bool)
+    for k in range(nm):
+        pend_any |= np.abs(r[k]) > eps[k]
+        assert abs(rsum[k] - np.abs(r[k].astype(np.float64)).sum()) <= 1e-9 * max(1.0, rsum[k])
+    assert np.array_equal(tr, pend_any.astype(np.uint16))
+    bits = bits_of(bm, n)
+    bounds = list(v0) + [n]
+    for c in range(len(v0)):
+        lst = np.sort(eng.chunk_list(c))
+        want = np.nonzero(bits[bounds[c]:bounds[c + 1]])[0] + bounds[c]
+        assert np.array_equal(lst, want), c
+    # the reference's own k_snapshot on identical inputs
+    L = ref_kernels()
+    dev = torch.device("cuda")
+    d_r = [torch.from_numpy(r[k]).to(dev) for k in range(nm)]
+    d_idx = torch.from_numpy(idx.view(np.int64)).to(dev)
+    d_cv0 = torch.from_numpy(v0).to(dev)
+    d_bm = torch.zeros((n + 31) // 32, dtype=torch.int32, device=dev)
+    d_cnt = torch.zeros(2 * len(v0), dtype=torch.int64, device=dev)
+    d_hot = torch.from_numpy(hot.view(np.int32)).to(dev)
+    d_hp = torch.zeros(1, dtype=torch.int64, device=dev)
+    rp = (C.c_void_p * 3)(*[t.data_ptr() for t in d_r], *([0] * (3 - nm)))
+    ep = (C.c_float * 3)(*[float(x) for x in eps], *([0.0] * (3 - nm)))
+    assert L.ref_snapshot(n, nm, rp, ep, d_idx.data_ptr(), d_cv0.data_ptr(), len(v0), d_bm.data_ptr(),
+                          d_cnt.data_ptr(), d_hot.data_ptr() if use_hot else None, d_hp.data_ptr(), None) == 0
+    assert np.array_equal(d_bm.cpu().numpy().view(np.uint32), bm)
+    assert np.array_equal(d_cnt.cpu().numpy().view(np.uint64), cnt)
+    assert int(d_hp.item()) == hp
+    # and the reference's k_compact per chunk, as sorted sets
+    out = torch.zeros(n, dtype=torch.int32, device=dev)
+    count = torch.zeros(1, dtype=torch.int32, device=dev)
+    for c in range(len(v0)):
+        assert L.ref_compact(int(bounds[c]), int(bounds[c + 1]), d_bm.data_ptr(), out.data_ptr(), count.data_ptr()) == 0
+        k = int(count.item())
+        assert np.array_equal(np.sort(out[:k].cpu().numpy()), np.sort(eng.chunk_list(c)))
+    eng.close()
+
+
+@pytest.mark.parametrize("measure", ["pr", "katz", "ev", "all"])
+def test_init_matches_reference_k_init(sample, measure):
+    n, idx, adj, env = sample
+    meas = meas_for(measure, env)
+    eng = make_engine(n, idx, adj, meas)
+    eng.init()
+    kinds = [int(meas.kind[i]) for i in range(meas.nm)]
+    L = ref_kernels()
+    dev = torch.device("cuda")
+    d_idx = torch.from_numpy(idx.view(np.int64)).to(dev)
+    for i, k in enumerate(kinds):
+        x = torch.zeros(n, dtype=torch.float32, device=dev)
+        r = torch.zeros(n, dtype=torch.float32, device=dev)
+        assert L.ref_init(n, d_idx.data_ptr(), x.data_ptr(), r.data_ptr(), k, float(env["BETA"]),
+                          float(np.float32(float(env["LAMBDA"])))) == 0
+        assert np.array_equal(eng.read(i), x.cpu().numpy())
+        assert np.array_equal(eng.read(i, residual=True), r.cpu().numpy())
+    eng.close()
+
+
+def solve_and_compare(n, idx, adj, measure, env=None, cap=None, use_graph=True, list_frac=0.5, **kw):
+    meas = meas_for(measure, env, **kw)
+    eng = make_engine(n, idx, adj, meas, cap)
+    st = eng.solve(list_frac=list_frac, use_graph=use_graph)
+    xs = eng.results()
+    res = []
+    names = ["pr", "katz", "ev"] if measure == "all" else [measure]
+    alpha = float(env["ALPHA"]) if env else kw.get("alpha")
+    for i, k in enumerate(names):
+        # converged: no residual above its threshold
+        r = eng.read(i, residual=True)
+        assert np.all(np.abs(r) <= np.float32(meas.eps[i])), k
+        ref = O.reference_solution(n, idx, adj, k, alpha=alpha)
+        res.append(O.compare(k, ref, xs[i]))
+    eng.close()
+    return st, res
+
+
+@pytest.mark.parametrize("measure", ["pr", "katz", "ev", "all"])
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_solve_sample_vs_fp64_oracle(sample, measure, use_graph):
+    n, idx, adj, env = sample
+    st, res = solve_and_compare(n, idx, adj, measure, env, use_graph=use_graph)
+    assert st.passes > 0 and st.pushed > 0
+    # CPU port of the reference engine on the same graph: same algorithm, so comparable error
+    kinds = ["pr", "katz", "ev"] if measure == "all" else [measure]
+    xs, _, _, _ = O.delta_push(n, idx, adj, kinds, alpha=float(env["ALPHA"]), lam=float(env["LAMBDA"]),
+                               eps_katz=float(env["EPS_KATZ"]), eps_ev=float(env["EPS_EV"]))
+    for i, k in enumerate(kinds):
+        ref = O.reference_solution(n, idx, adj, k, alpha=float(env["ALPHA"]))
+        port = O.compare(k, ref, xs[i])
+        assert res[i]["l1_rel"] <= 1.5 * port["l1_rel"] + 1e-6, (k, res[i], port)
+        assert res[i]["top100"] >= 95
+
+
+def test_solve_rmat16_pagerank(rmat16):
+    n, idx, adj = rmat16
+    st, res = solve_and_compare(n, idx, adj, "pr")
+    assert res[0]["l1_rel"] < 0.04 and res[0]["top1000"] >= 980, res
+    assert st.pushed > 5 * len(adj)
+
+
+def test_solve_multi_chunk_host_driven_push(rmat12):
+    """The host-driven pass of the CLI: snapshot, host fetch plan, push of
+    every resident chunk in one launch, until nothing is pending."""
+    n, idx, adj = rmat12
+    meas = X.measures("pr")
+    eng = make_engine(n, idx, adj, meas, cap=5000)
+    eng.init()
+    passes = 0
+    while True:
+        cnt, hp, rs = eng.snapshot()
+        if cnt[0::2].sum() == 0:
+            break
+        mode = (cnt[0::2] > 0).astype(np.uint8)
+        eng.push_cached(mode, cnt, 0.5)
+        eng.sync()
+        passes += 1
+        assert passes < 500
+    x = eng.read(0)
+    ref = O.reference_solution(n, idx, adj, "pr")
+    c = O.compare("pr", ref, x)
+    assert c["l1_rel"] < 0.05 and c["top100"] >= 95
+    eng.close()
+
+
+def test_rmat_generator_bitexact_vs_oracle():
+    for scale, ef, seed, sym in [(10, 16, 1, True), (12, 8, 3, True), (11, 16, 4, False)]:
+        g = X.DeviceGraph(scale, ef, seed, symmetric=sym, weights=not sym)
+        idx, adj, w = g.download()
+        n, idx_o, adj_o = O.rmat_graph(scale, ef, seed, symmetric=sym)
+        assert g.n == n and g.m == len(adj_o)
+        assert np.array_equal(idx, idx_o) and np.array_equal(adj[:g.m], adj_o)
+        if not sym:
+            assert np.array_equal(w[:g.m], O.rmat_weights(g.m, seed))
+        g.close()
