@@ -160,7 +160,7 @@ class Engine:
     def stats(self, with_log=False):
         st = Stats()
         if with_log:
-            cap = 1 << 16
+            cap = 1 << 17
             log = (PassLog * cap)()
             call("excent_engine_stats", self.h, C.byref(st), log, cap)
             return st, [log[i] for i in range(min(st.passes, cap))]

@@ -705,7 +705,7 @@ static int engine_setup(excent_engine* e, int device, int n, ull m, const excent
     e->hub_cap[0] = 2 * (m / HUB_SEG) + 64;
     EX_ALLOC(e->d_hubq[0], e->hub_cap[0] * sizeof(HubSeg));
     EX_ALLOC(e->d_hubcnt, 3 * sizeof(ull));
-    e->log_cap = 1 << 16;
+    e->log_cap = 1 << 17;
     EX_ALLOC(e->d_log, (size_t)e->log_cap * sizeof(PassRec));
     if (e->L == 4) EX_ALLOC(e->d_tmp, (size_t)n * sizeof(float));
     EX_HALLOC(e->h_cnt, 2 * (size_t)nc * sizeof(ull));
