@@ -78,6 +78,23 @@ PROTOS = [
     ("excent_params_fp64", C.c_int, [C.c_int, C.c_int, vp, vp, C.c_double, f64p]),
     ("excent_reference_fp64", C.c_int, [C.c_int, C.c_int, vp, vp, C.c_int, C.c_double, C.c_double, C.c_double,
                                         C.c_int, f64p, C.POINTER(C.c_int)]),
+    ("excent_device_info", C.c_int, [C.c_int, vp]),
+    ("excent_egr_open", C.c_int, [C.c_char_p, C.c_int, C.c_int, C.POINTER(vp)]),
+    ("excent_egr_close", C.c_int, [vp]),
+    ("excent_egr_info", C.c_int, [vp, C.POINTER(C.c_int), u64p, C.POINTER(C.c_int)]),
+    ("excent_egr_read_offsets", C.c_int, [vp, u64, u64, vp]),
+    ("excent_egr_read_edges", C.c_int, [vp, u64, u64, vp]),
+    ("excent_egr_prefetch", C.c_int, [vp, vp, C.c_int, u64p, u64p]),
+    ("excent_egr_drop_cache", C.c_int, [vp, u64, u64, u64, u64]),
+    ("excent_chunk_cap", C.c_uint64, [u64, C.c_double, C.c_double, C.c_double]),
+    ("excent_plan_chunks", C.c_int, [C.c_int, vp, u64, C.POINTER(C.c_int), vp, C.c_int]),
+    ("excent_cache_chunks", C.c_int, [C.c_int, vp, u64, u64, C.POINTER(C.c_int)]),
+    ("excent_hot_select", C.c_int, [C.c_int, vp, u64, vp, C.POINTER(C.c_int), vp, vp, vp, u64p]),
+    ("excent_fetch_plan", C.c_int, [C.c_int, vp, vp, vp, vp, C.c_double, C.c_int, C.c_int, vp, vp, vp, u64p, u64p,
+                                    C.POINTER(C.c_int)]),
+    ("excent_gather_list", C.c_int, [C.c_int, C.c_int, vp, vp, vp, vp, C.POINTER(C.c_int)]),
+    ("excent_tau", C.c_double, [C.c_double, vp, vp]),
+    ("excent_cli_main", C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
     ("excent_rmat_generate", C.c_int, [C.c_int, C.c_int, C.c_int, u64, C.c_double, C.c_double, C.c_double,
                                        C.c_int, C.c_int, C.POINTER(vp)]),
     ("excent_dgraph_info", C.c_int, [vp, C.POINTER(C.c_int), u64p]),

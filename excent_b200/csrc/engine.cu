@@ -1332,6 +1332,20 @@ extern "C" int excent_engine_write(excent_engine* e, int i, const float* x, cons
     return EXCENT_OK;
 }
 
+extern "C" int excent_device_info(int device, excent_device_info_t* out) {
+    EX_CHECK_ARG(out, "null argument");
+    EX_CUDA(cudaSetDevice(device));
+    size_t f = 0, t = 0;
+    EX_CUDA(cudaMemGetInfo(&f, &t));
+    out->free_bytes = f;
+    out->total_bytes = t;
+    EX_CUDA(cudaDeviceGetAttribute(&out->integrated, cudaDevAttrIntegrated, device));
+    EX_CUDA(cudaDeviceGetAttribute(&out->sms, cudaDevAttrMultiProcessorCount, device));
+    EX_CUDA(cudaDeviceGetAttribute(&out->cc_major, cudaDevAttrComputeCapabilityMajor, device));
+    EX_CUDA(cudaDeviceGetAttribute(&out->cc_minor, cudaDevAttrComputeCapabilityMinor, device));
+    return EXCENT_OK;
+}
+
 extern "C" int excent_engine_stream(excent_engine* e, void** stream) {
     EX_CHECK_ARG(e && stream, "null argument");
     *stream = (void*)e->s_main;

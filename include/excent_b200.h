@@ -209,6 +209,80 @@ int excent_engine_profile_read(excent_engine* e, double* ms, unsigned long long*
 /* Number of device kernel launches this engine issued so far. */
 int excent_engine_launches(excent_engine* e, unsigned long long* launches);
 
+/* Free / total device memory, integrated flag, SM count and compute
+ * capability of `device` (the reference queries these at src/excent.cu:370,
+ * 375, 404). */
+typedef struct excent_device_info_t {
+    unsigned long long free_bytes, total_bytes;
+    int integrated, sms, cc_major, cc_minor;
+} excent_device_info_t;
+int excent_device_info(int device, excent_device_info_t* out);
+
+/* ------------------------------------------------------------ EGR files */
+
+/* A storage-resident EGR graph (README.md:136-146): the header is parsed
+ * (int32 offsets, or int64 when the edge count is -1), the file is mapped,
+ * offsets are validated (monotone, spanning [0, m]) and kept mapped or in
+ * RAM. A truncated file, a bad header or failed reads return
+ * EXCENT_ERR_IO instead of exiting. Replaces StaticGraph
+ * (include/StaticGraph.h:29-68). */
+typedef struct excent_egr excent_egr;
+int excent_egr_open(const char* path, int io_threads, int offsets_in_ram, excent_egr** out);
+int excent_egr_close(excent_egr* g);
+int excent_egr_info(excent_egr* g, int* n, unsigned long long* m, int* wide);
+/* Offsets idx[v0 .. v0+count) as uint64 (include/StaticGraph.h:81-84). */
+int excent_egr_read_offsets(excent_egr* g, unsigned long long v0, unsigned long long count, unsigned long long* dst);
+/* Edges [e0, e1) by parallel pread in 8 MiB pieces (include/StaticGraph.h:86-88, 160-170). */
+int excent_egr_read_edges(excent_egr* g, unsigned long long e0, unsigned long long e1, int32_t* dst);
+/* Page-deduplicated readahead of k adjacency lists; returns the pages and
+ * runs requested (include/StaticGraph.h:90-114). */
+int excent_egr_prefetch(excent_egr* g, const int32_t* vids, int k, unsigned long long* pages, unsigned long long* runs);
+/* Evict a chunk's edges and offsets from the page cache (include/StaticGraph.h:116-126). */
+int excent_egr_drop_cache(excent_egr* g, unsigned long long e0, unsigned long long e1, unsigned long long v0,
+                          unsigned long long v1);
+
+/* ------------------------------------------------------------ host planner */
+
+/* Chunk edge cap: chunk_medges * 1e6 if > 0, else clamp(ceil(m / target_chunks),
+ * min_chunk_medges * 1e6, 64e6) (src/excent.cu:321-326). */
+unsigned long long excent_chunk_cap(unsigned long long m, double chunk_medges, double target_chunks,
+                                    double min_chunk_medges);
+/* Greedy contiguous chunks of <= cap edges, >= 1 vertex each; out gets 4
+ * entries {v0, v1, e0, e1} per chunk (NULL: count only)
+ * (include/StaticGraph.h:128-139). */
+int excent_plan_chunks(int n, const unsigned long long* off, unsigned long long cap, int* nc,
+                       unsigned long long* out, int out_cap);
+/* Leading chunks that fit in free - reserve bytes (src/excent.cu:410-421). */
+int excent_cache_chunks(int nc, const unsigned long long* chunk_edges, unsigned long long free_bytes,
+                        unsigned long long reserve, int* resident);
+/* Degree cache selection under a byte budget, by degree threshold or by a
+ * uint16 score per vertex (--hot-rank); ids ascending, offsets nh+1, bitmap
+ * ceil(n/32) words (src/excent.cu:428-491). Output arrays may be NULL to
+ * count only (size them with n, n+1 and ceil(n/32)). */
+int excent_hot_select(int n, const unsigned long long* off, unsigned long long budget, const uint16_t* score, int* nh,
+                      int32_t* ids, unsigned long long* hoff, uint32_t* bits, unsigned long long* threshold);
+/* Per-chunk mode 0 skip, 1 resident, 2 stream, 3 gather, with the pending
+ * and demand totals and whether the bitmap is needed (src/excent.cu:666-678). */
+int excent_fetch_plan(int nc, const unsigned long long* chunk_edges, const unsigned long long* cnt,
+                      const uint8_t* resident, const uint8_t* loaded, double stream_ratio, int hot_mode, int pass,
+                      const int* hlo, const int* hhi, uint8_t* mode, unsigned long long* pend_v,
+                      unsigned long long* demand, int* need_bitmap);
+/* Ascending pending ids of [v0, v1) from the bitmap and the prefix sums of
+ * their degrees (src/excent.cu:711-723). */
+int excent_gather_list(int v0, int v1, const uint32_t* bitmap, const unsigned long long* idx, int32_t* vids,
+                       unsigned long long* off, int* k);
+/* Stream/gather crossover tau from one stream time and three gather times at
+ * demand fractions f[3], clamped to [0.005, 1] (src/excent.cu:566-572). */
+double excent_tau(double t_stream, const double* t_g, const double* f);
+
+/* ------------------------------------------------------------ command line */
+
+/* The excent command line (argv as bin/excent takes it: graph.egr then the
+ * flags of src/excent.cu:269-298, plus --device N, --gpu-budget-gb X and
+ * --device-loop). Prints the reference's stdout lines; returns the process
+ * exit code (0, or 1 on a usage or run error). */
+int excent_cli_main(int argc, char** argv);
+
 /* ------------------------------------------------------------ FP64 tools */
 
 /* Given constants of a symmetric device-resident graph (offsets and lists
