@@ -42,6 +42,15 @@ CONFIGS = {
 }
 
 
+T_START = time.perf_counter()
+
+
+def log(msg):
+    """Progress on stderr (the JSON line alone goes to stdout)."""
+    sys.stderr.write("[bench %7.1fs] %s\n" % (time.perf_counter() - T_START, msg))
+    sys.stderr.flush()
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -131,9 +140,11 @@ def run_ours(a, world, rank, local, dist):
     g = X.DeviceGraph(scale, ef, seed, device=local)
     n, m = g.n, g.m
     d_idx, d_adj, _ = g.device_ptrs()
+    log(f"graph scale {scale}: n={n} m={m}")
     if measure == "all":
         par = X.params_fp64(n, d_idx, d_adj, device=local)
         lam = par["lambda"]
+        log(f"lambda1 {lam:.6f} after {par['sweeps']} sweeps")
         meas = X.measures("all", alpha=0.9 / lam, beta=1.0, lam=lam, eps_pr=1e-2, eps_katz=1e-6, eps_ev=1e-6)
     else:
         lam = None
@@ -149,7 +160,8 @@ def run_ours(a, world, rank, local, dist):
     eng.upload_device(d_idx, d_adj)
     use_graph = not a.no_graph
     for _ in range(a.warmup):
-        eng.solve(use_graph=use_graph)
+        s = eng.solve(use_graph=use_graph)
+        log(f"warmup solve: {s.passes} passes, {s.pushed} entries pushed")
     st = torch.cuda.ExternalStream(eng.stream())
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     clocks = ClockSampler(local)
@@ -180,6 +192,7 @@ def run_ours(a, world, rank, local, dist):
     else:
         pushed_all = float(pushed)
     value = pushed_all / t / 1e9
+    log(f"timed: {a.steps} solves in {t:.3f}s, {value:.3f} GTEPS")
 
     # end to end through the C ABI: host buffers in, host results out
     outs = [torch.empty(n, dtype=torch.float32, pin_memory=True) for _ in range(nm)]
@@ -210,6 +223,7 @@ def run_ours(a, world, rank, local, dist):
         dist.all_reduce(pp)
         e_pushed = float(pp.item())
 
+    log(f"e2e: {a.steps} solves in {te:.3f}s")
     # roofline of the dominant kernel (push + its hub tail), per-kernel events on a profiled solve
     eng.profile(True)
     s, log = eng.solve(use_graph=False), None
@@ -254,6 +268,7 @@ def run_ours(a, world, rank, local, dist):
         "clocks": ck,
         "gpu_launches": int(launches),
     }
+    log(f"profiled solve: {prof}")
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(n, idx_np, h_adj.numpy()[:m], meas, measure, lam)
     g.close()

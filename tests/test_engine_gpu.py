@@ -242,3 +242,26 @@ def test_rmat_generator_bitexact_vs_oracle():
         if not sym:
             assert np.array_equal(w[:g.m], O.rmat_weights(g.m, seed))
         g.close()
+
+
+@pytest.mark.parametrize("measure", ["pr", "katz", "ev", "all"])
+def test_error_no_looser_than_reference_engine(sample, measure):
+    """The reference engine's own result dumps on the sample (built from its
+    source and run on a B200, committed under tests/golden/) against the
+    reference's FP64 oracle vectors: our L1 and max errors must not be looser."""
+    from conftest import GOLDEN
+    n, idx, adj, env = sample
+    names = ["pr", "katz", "ev"] if measure == "all" else [measure]
+    meas = meas_for(measure, env)
+    eng = make_engine(n, idx, adj, meas)
+    eng.solve()
+    for i, k in enumerate(names):
+        p = os.path.join(GOLDEN, f"sample_excent_{measure}_{k}.f32")
+        ref = np.fromfile(os.path.join(GOLDEN, f"sample_ref_{k}.f64"))
+        theirs = O.compare(k, ref, np.fromfile(p, dtype=np.float32))
+        ours = O.compare(k, ref, eng.read(i))
+        print(measure, k, "ours", ours, "reference engine", theirs)
+        assert ours["l1_rel"] <= theirs["l1_rel"] * 1.02, (k, ours, theirs)
+        assert ours["max_abs"] <= theirs["max_abs"] * 1.10, (k, ours, theirs)
+        assert ours["top1000"] >= theirs["top1000"] - 3
+    eng.close()
