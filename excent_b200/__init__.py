@@ -269,3 +269,77 @@ class DeviceGraph:
             self.close()
         except Exception:
             pass
+
+
+class Batch:
+    """B personalized PageRank (kind "ppr") or Katz ("katz") solves at once on a
+    device-resident graph (excent_batch_*), residuals vertex-major [n][B]."""
+
+    def __init__(self, n, m, d_idx, d_adj, B, kind="ppr", d_or_alpha=0.85, device=0):
+        h = C.c_void_p()
+        k = {"ppr": 0, "katz": 1}[kind]
+        call("excent_batch_create", int(device), int(n), int(m), _ptr(d_idx), _ptr(d_adj), int(B), k,
+             float(d_or_alpha), C.byref(h))
+        self.h, self.n, self.B, self.kind = h, int(n), int(B), kind
+
+    def seed(self, seeds, values, eps):
+        """seeds: list of vertex-id arrays (one per lane); values: matching arrays or scalars; eps per lane."""
+        nq = len(seeds)
+        off = np.zeros(nq + 1, dtype=np.int32)
+        off[1:] = np.cumsum([len(s) for s in seeds])
+        vids = np.ascontiguousarray(np.concatenate(seeds) if nq else np.zeros(0), dtype=np.int32)
+        vals = np.ascontiguousarray(np.concatenate([np.broadcast_to(np.asarray(v, dtype=np.float32), (len(s),))
+                                                    for s, v in zip(seeds, values)]) if nq else np.zeros(0),
+                                    dtype=np.float32)
+        e = np.ascontiguousarray(np.broadcast_to(np.asarray(eps, dtype=np.float32), (nq,)))
+        call("excent_batch_seed", self.h, nq, _ptr(off), _ptr(vids) if len(vids) else None,
+             _ptr(vals) if len(vals) else None, _ptr(e))
+
+    def solve(self, max_passes=100000, use_graph=True):
+        call("excent_batch_solve", self.h, int(max_passes), int(use_graph))
+        return self.stats()
+
+    def stats(self):
+        p = C.c_int()
+        v, e, u = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        call("excent_batch_stats", self.h, C.byref(p), C.byref(v), C.byref(e), C.byref(u))
+        return {"passes": p.value, "pushed_vertices": v.value, "pushed_edges": e.value, "lane_updates": u.value}
+
+    def read(self, lane, residual=False, out=None):
+        if out is None:
+            out = np.empty(self.n, dtype=np.float32)
+        call("excent_batch_read", self.h, int(lane), int(residual), _ptr(out))
+        return out
+
+    def stream(self):
+        s = C.c_void_p()
+        call("excent_batch_stream", self.h, C.byref(s))
+        return s.value or 0
+
+    def launches(self):
+        v = C.c_uint64()
+        call("excent_batch_launches", self.h, C.byref(v))
+        return v.value
+
+    def close(self):
+        if self.h:
+            call("excent_batch_destroy", self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def seed_engine(eng, vids, vals):
+    """Zero a single-measure engine and seed residuals (excent_engine_seed)."""
+    vids = np.ascontiguousarray(vids, dtype=np.int32)
+    vals = np.ascontiguousarray(np.broadcast_to(np.asarray(vals, dtype=np.float32), vids.shape))
+    call("excent_engine_seed", eng.h, len(vids), _ptr(vids), _ptr(vals))
+
+
+def resume(eng, list_frac=0.5, max_passes=100000, use_graph=True):
+    call("excent_engine_resume", eng.h, float(list_frac), int(max_passes), int(use_graph))
+    return eng.stats()

@@ -66,6 +66,16 @@ PROTOS = [
     ("excent_engine_push_hot", C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
     ("excent_engine_sync", C.c_int, [vp]),
     ("excent_engine_solve", C.c_int, [vp, C.c_double, C.c_int, C.c_int]),
+    ("excent_engine_resume", C.c_int, [vp, C.c_double, C.c_int, C.c_int]),
+    ("excent_engine_seed", C.c_int, [vp, C.c_int, vp, vp]),
+    ("excent_batch_create", C.c_int, [C.c_int, C.c_int, u64, vp, vp, C.c_int, C.c_int, C.c_double, C.POINTER(vp)]),
+    ("excent_batch_destroy", C.c_int, [vp]),
+    ("excent_batch_seed", C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
+    ("excent_batch_solve", C.c_int, [vp, C.c_int, C.c_int]),
+    ("excent_batch_stats", C.c_int, [vp, C.POINTER(C.c_int), u64p, u64p, u64p]),
+    ("excent_batch_read", C.c_int, [vp, C.c_int, C.c_int, vp]),
+    ("excent_batch_stream", C.c_int, [vp, C.POINTER(vp)]),
+    ("excent_batch_launches", C.c_int, [vp, u64p]),
     ("excent_engine_stats", C.c_int, [vp, C.POINTER(Stats), C.POINTER(PassLog), C.c_int]),
     ("excent_engine_read", C.c_int, [vp, C.c_int, C.c_int, vp, u64, u64]),
     ("excent_engine_write", C.c_int, [vp, C.c_int, vp, vp]),

@@ -854,6 +854,16 @@ extern "C" int excent_engine_read_trace(excent_engine* e, uint16_t* out) {
     return EXCENT_OK;
 }
 
+static int reset_counters(excent_engine* e) {
+    EX_CUDA(cudaMemsetAsync(e->d_ctrl, 0, sizeof(Ctrl), e->s_main));
+    EX_CUDA(cudaMemsetAsync(e->d_hubcnt, 0, 3 * sizeof(ull), e->s_main));
+    EX_CUDA(cudaMemsetAsync(e->d_cnt, 0, 2 * (size_t)e->nc * sizeof(ull), e->s_main));
+    if (e->d_trace && e->trace_on) EX_CUDA(cudaMemsetAsync(e->d_trace, 0, (size_t)e->n * sizeof(uint16_t), e->s_main));
+    e->hot_skip = false;
+    e->n_list = e->n_range = 0;
+    return EXCENT_OK;
+}
+
 static int init_state(excent_engine* e) {
     const excent_measures& ms = e->meas;
     const int g = e->sms * 8;
@@ -865,13 +875,7 @@ static int init_state(excent_engine* e) {
                                                ms.kind[0], ms.kind[1], ms.kind[2], (float)ms.beta, (float)ms.lambda);
     e->launches++;
     EX_CUDA(cudaGetLastError());
-    EX_CUDA(cudaMemsetAsync(e->d_ctrl, 0, sizeof(Ctrl), e->s_main));
-    EX_CUDA(cudaMemsetAsync(e->d_hubcnt, 0, 3 * sizeof(ull), e->s_main));
-    EX_CUDA(cudaMemsetAsync(e->d_cnt, 0, 2 * (size_t)e->nc * sizeof(ull), e->s_main));
-    e->hot_skip = false;
-    if (e->d_trace && e->trace_on) EX_CUDA(cudaMemsetAsync(e->d_trace, 0, (size_t)e->n * sizeof(uint16_t), e->s_main));
-    e->n_list = e->n_range = 0;
-    return EXCENT_OK;
+    return reset_counters(e);
 }
 
 extern "C" int excent_engine_init(excent_engine* e) {
@@ -1226,7 +1230,43 @@ static int build_graph(excent_engine* e, double list_frac, int max_passes) {
     return EXCENT_OK;
 }
 
+static int solve_impl(excent_engine* e, double list_frac, int max_passes, int use_graph, bool init);
+
 extern "C" int excent_engine_solve(excent_engine* e, double list_frac, int max_passes, int use_graph) {
+    return solve_impl(e, list_frac, max_passes, use_graph, true);
+}
+
+extern "C" int excent_engine_resume(excent_engine* e, double list_frac, int max_passes, int use_graph) {
+    return solve_impl(e, list_frac, max_passes, use_graph, false);
+}
+
+__global__ void k_seed(int k, const int* vids, const float* vals, float* r) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) atomicAdd(&r[vids[i]], vals[i]);
+}
+
+extern "C" int excent_engine_seed(excent_engine* e, int k, const int32_t* vids, const float* vals) {
+    EX_CHECK_ARG(e && k >= 0 && (k == 0 || (vids && vals)), "bad argument");
+    EX_CHECK_ARG(e->L == 1, "seeded solves need a single-measure engine");
+    for (int i = 0; i < k; i++) EX_CHECK_ARG(vids[i] >= 0 && vids[i] < e->n, "seed vertex %d out of range", vids[i]);
+    EX_CUDA(cudaSetDevice(e->dev));
+    EX_CUDA(cudaMemsetAsync(e->d_x, 0, (size_t)e->n * sizeof(float), e->s_main));
+    EX_CUDA(cudaMemsetAsync(e->d_r, 0, (size_t)e->n * sizeof(float), e->s_main));
+    if (k) {
+        // seed lists ride in the pending-list buffer (n ints), which the next snapshot rewrites
+        EX_CHECK_ARG((size_t)k * 2 <= (size_t)e->n, "too many seeds (%d) for n = %d", k, e->n);
+        EX_CUDA(cudaMemcpyAsync(e->d_list, vids, (size_t)k * sizeof(int), cudaMemcpyHostToDevice, e->s_main));
+        EX_CUDA(cudaMemcpyAsync(e->d_list + k, vals, (size_t)k * sizeof(float), cudaMemcpyHostToDevice, e->s_main));
+        k_seed<<<std::min(1024, (k + 255) / 256), 256, 0, e->s_main>>>(k, e->d_list, (const float*)(e->d_list + k),
+                                                                       (float*)e->d_r);
+        e->launches++;
+        EX_CUDA(cudaGetLastError());
+    }
+    EX_TRY(reset_counters(e));
+    EX_CUDA(cudaStreamSynchronize(e->s_main));
+    return EXCENT_OK;
+}
+
+static int solve_impl(excent_engine* e, double list_frac, int max_passes, int use_graph, bool init) {
     EX_CHECK_ARG(e, "null engine");
     EX_CHECK_ARG(max_passes >= 0 && max_passes < e->log_cap, "max_passes must be < %d", e->log_cap);
     for (int c = 0; c < e->nc; c++)
@@ -1234,7 +1274,8 @@ extern "C" int excent_engine_solve(excent_engine* e, double list_frac, int max_p
     EX_CUDA(cudaSetDevice(e->dev));
     std::vector<uint8_t> cm(e->nc, 1);
     EX_CUDA(cudaMemcpyAsync(e->d_cmode, cm.data(), e->nc, cudaMemcpyHostToDevice, e->s_main));
-    EX_TRY(init_state(e));
+    if (init) EX_TRY(init_state(e));
+    else EX_TRY(reset_counters(e));
     if (use_graph) {
         EX_TRY(build_graph(e, list_frac, max_passes));
         EX_CUDA(cudaGraphLaunch(e->gexec, e->s_main));

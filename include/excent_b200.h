@@ -164,6 +164,14 @@ int excent_engine_sync(excent_engine* e);
  * Per-pass log and totals are kept for excent_engine_stats. */
 int excent_engine_solve(excent_engine* e, double list_frac, int max_passes, int use_graph);
 
+/* Same as excent_engine_solve but from the current values and residuals
+ * (no k_init): for seeded or restarted solves. */
+int excent_engine_resume(excent_engine* e, double list_frac, int max_passes, int use_graph);
+/* Single-measure engines: zero values and residuals, then add vals[i] to the
+ * residual of vids[i] (a personalized start, e.g. (1-d)/|S| on a seed set S
+ * for personalized PageRank). Follow with excent_engine_resume. */
+int excent_engine_seed(excent_engine* e, int k, const int32_t* vids, const float* vals);
+
 typedef struct excent_pass_log {
     unsigned long long pending;   /* pending vertices at the snapshot */
     unsigned long long demand;    /* their total degree */
@@ -282,6 +290,34 @@ double excent_tau(double t_stream, const double* t_g, const double* f);
  * --device-loop). Prints the reference's stdout lines; returns the process
  * exit code (0, or 1 on a usage or run error). */
 int excent_cli_main(int argc, char** argv);
+
+/* ------------------------------------------------------------ batched solves */
+
+/* B personalized PageRank (kind EXCENT_PR: weight d / deg) or Katz (kind
+ * EXCENT_KATZ: weight alpha) solves at once on a cached graph given by device
+ * pointers (offsets n+1, lists m; symmetric for the PageRank reading).
+ * Residuals and values are vertex-major float32 [n][B], B in {32, 64, 128,
+ * 256}. No reference counterpart: the reference runs one solve per process. */
+typedef struct excent_batch excent_batch;
+int excent_batch_create(int device, int n, unsigned long long m, const unsigned long long* d_idx, const int32_t* d_adj,
+                        int B, int kind, double d_or_alpha, excent_batch** out);
+int excent_batch_destroy(excent_batch* b);
+/* Reset all lanes to zero and seed lanes 0..nq-1: lane q adds vals[i] to the
+ * residual of vids[i] for i in [lane_off[q], lane_off[q+1]); eps[q] is its
+ * absolute threshold. Lanes >= nq stay idle. */
+int excent_batch_seed(excent_batch* b, int nq, const int* lane_off, const int32_t* vids, const float* vals,
+                      const float* eps);
+/* Passes until no lane of any vertex is pending (or max_passes); with
+ * use_graph all passes run as one CUDA graph with a conditional while node. */
+int excent_batch_solve(excent_batch* b, int max_passes, int use_graph);
+/* Passes, pushed vertices, pushed adjacency entries, and 16-byte lane-group
+ * reductions issued by the last solve. */
+int excent_batch_stats(excent_batch* b, int* passes, unsigned long long* pushed_vertices,
+                       unsigned long long* pushed_edges, unsigned long long* lane_updates);
+/* Values (or residuals) of lane q for all n vertices, to host float32. */
+int excent_batch_read(excent_batch* b, int lane, int residual, float* out);
+int excent_batch_stream(excent_batch* b, void** stream);
+int excent_batch_launches(excent_batch* b, unsigned long long* launches);
 
 /* ------------------------------------------------------------ FP64 tools */
 
