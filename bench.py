@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--scale", type=int, default=None, help="override the graph scale (smaller test runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="host-driven pass loop instead of the CUDA graph")
+    ap.add_argument("--ev-init", default="fp64", choices=["fp64", "reference"],
+                    help="eigenvector initial residual from the FP64 lambda1 (default) or from lambda1 rounded to "
+                         "float as the reference does")
     return ap.parse_args()
 
 
@@ -145,7 +148,8 @@ def run_ours(a, world, rank, local, dist):
         par = X.params_fp64(n, d_idx, d_adj, device=local)
         lam = par["lambda"]
         log(f"lambda1 {lam:.6f} after {par['sweeps']} sweeps")
-        meas = X.measures("all", alpha=0.9 / lam, beta=1.0, lam=lam, eps_pr=1e-2, eps_katz=1e-6, eps_ev=1e-6)
+        meas = X.measures("all", alpha=0.9 / lam, beta=1.0, lam=lam, eps_pr=1e-2, eps_katz=1e-6, eps_ev=1e-6,
+                          ev_init_fp64=a.ev_init == "fp64")
     else:
         lam = None
         meas = X.measures("pr", eps_pr=1e-2)
@@ -254,7 +258,8 @@ def run_ours(a, world, rank, local, dist):
                    "eps": [float(meas.eps[i]) for i in range(nm)], "passes_per_solve": passes[-1],
                    "pushed_per_solve": int(pushed / a.steps), "time_to_eps_ms": round(t / a.steps * 1e3, 3),
                    "l2_note": "inputs larger than L2 (edge cache %.2f GB)" % (m * 4 / 1e9),
-                   "cuda_graph": use_graph, "parallelism": f"{world} independent replicas"},
+                   "cuda_graph": use_graph, "parallelism": f"{world} independent replicas",
+                   "ev_init": a.ev_init},
         "e2e": {"value": round(e_pushed / te / 1e9, 4), "unit": "GTEPS", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": round(te / a.steps * 1e3, 3),
                 "wall_ms_per_step": round(te_wall / a.steps * 1e3, 3)},

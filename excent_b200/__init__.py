@@ -37,11 +37,18 @@ def _tp(a, t):
     return C.cast(_ptr(a), t) if a is not None else C.cast(0, t)
 
 
-def measures(measure, alpha=-1.0, beta=1.0, lam=-1.0, eps_pr=0.01, eps_katz=-1.0, eps_ev=-1.0) -> Measures:
-    """--measure pr|katz|ev|all with --alpha/--beta/--lambda/--eps-* (src/excent.cu:292-316, 344-351)."""
+EV_INIT_FP64 = 1
+
+
+def measures(measure, alpha=-1.0, beta=1.0, lam=-1.0, eps_pr=0.01, eps_katz=-1.0, eps_ev=-1.0,
+             ev_init_fp64=False) -> Measures:
+    """--measure pr|katz|ev|all with --alpha/--beta/--lambda/--eps-* (src/excent.cu:292-316, 344-351).
+    ev_init_fp64: eigenvector initial residual from the FP64 lambda1 (the reference rounds it to float)."""
     M = Measures()
     call("excent_measures_make", C.byref(M), measure.encode(), float(alpha), float(beta), float(lam),
          float(eps_pr), float(eps_katz), float(eps_ev))
+    if ev_init_fp64:
+        M.flags |= EV_INIT_FP64
     return M
 
 

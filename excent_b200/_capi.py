@@ -26,7 +26,7 @@ vp = C.c_void_p
 
 class Measures(C.Structure):
     _fields_ = [("nm", C.c_int), ("kind", C.c_int * 3), ("eps", C.c_float * 3), ("scale", C.c_float * 3),
-                ("divdeg", C.c_int * 3), ("beta", C.c_double), ("lambda_", C.c_double)]
+                ("divdeg", C.c_int * 3), ("beta", C.c_double), ("lambda_", C.c_double), ("flags", C.c_int)]
 
 
 class PassLog(C.Structure):
@@ -85,6 +85,17 @@ PROTOS = [
     ("excent_engine_stream", C.c_int, [vp, C.POINTER(vp)]),
     ("excent_engine_profile", C.c_int, [vp, C.c_int]),
     ("excent_engine_profile_read", C.c_int, [vp, f64p, u64p]),
+    ("excent_wgraph_create", C.c_int, [C.c_int, C.c_int, u64, vp, vp, vp, C.POINTER(vp)]),
+    ("excent_wgraph_destroy", C.c_int, [vp]),
+    ("excent_wgraph_set_weights", C.c_int, [vp, vp]),
+    ("excent_wgraph_forward", C.c_int, [vp, C.c_int, C.c_double, vp, C.c_float, C.c_int, vp, C.POINTER(C.c_int),
+                                        u64p]),
+    ("excent_wgraph_vjp", C.c_int, [vp, vp, C.c_float, C.c_int, vp, vp, C.POINTER(C.c_int), u64p]),
+    ("excent_wgraph_lambda", C.c_int, [vp, vp]),
+    ("excent_wgraph_loss_fp64", C.c_int, [vp, C.c_int, C.c_double, vp, vp, C.c_longlong, C.c_double, C.c_double,
+                                          f64p]),
+    ("excent_wgraph_grad_fp64", C.c_int, [vp, C.c_int, C.c_double, vp, vp, C.c_double, vp, vp]),
+    ("excent_wgraph_stream", C.c_int, [vp, C.POINTER(vp)]),
     ("excent_params_fp64", C.c_int, [C.c_int, C.c_int, vp, vp, C.c_double, f64p]),
     ("excent_reference_fp64", C.c_int, [C.c_int, C.c_int, vp, vp, C.c_int, C.c_double, C.c_double, C.c_double,
                                         C.c_int, f64p, C.POINTER(C.c_int)]),

@@ -110,7 +110,7 @@ struct PushArgs {
 
 template <int L>
 __global__ void k_init(int n, const ull* idx, typename Lane<L>::T* x, typename Lane<L>::T* r, int nm, int k0, int k1,
-                       int k2, float beta, float lambda) {
+                       int k2, float beta, double lambda) {
     const int kind[3] = {k0, k1, k2};
     for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n;
          v += (long long)gridDim.x * blockDim.x) {
@@ -122,7 +122,7 @@ __global__ void k_init(int n, const ull* idx, typename Lane<L>::T* x, typename L
             // src/excent.cu:43-45
             if (kind[k] == 0) { xs[k] = 0.f; rs[k] = 1.f - 0.85f; }
             else if (kind[k] == 1) { xs[k] = 0.f; rs[k] = beta; }
-            else { xs[k] = 1.f; rs[k] = (float)((double)(idx[v + 1] - idx[v]) / lambda - 1.0); }
+            else { xs[k] = 1.f; rs[k] = (float)((double)(idx[v + 1] - idx[v]) / lambda - 1.0); }  // lambda: see init_state
         }
         if constexpr (L == 1) { x[v] = xs[0]; r[v] = rs[0]; }
         else { x[v] = make_float4(xs[0], xs[1], xs[2], 0.f); r[v] = make_float4(rs[0], rs[1], rs[2], 0.f); }
@@ -756,6 +756,7 @@ extern "C" int excent_measures_make(excent_measures* out, const char* measure, d
     }
     M.beta = beta;
     M.lambda = lambda;
+    M.flags = 0;
     *out = M;
     return EXCENT_OK;
 }
@@ -866,13 +867,16 @@ static int reset_counters(excent_engine* e) {
 
 static int init_state(excent_engine* e) {
     const excent_measures& ms = e->meas;
+    // The reference passes lambda1 to k_init as a float (src/excent.cu:41, 372);
+    // EXCENT_EV_INIT_FP64 keeps the FP64 value.
+    const double lam = (ms.flags & EXCENT_EV_INIT_FP64) ? ms.lambda : (double)(float)ms.lambda;
     const int g = e->sms * 8;
     if (e->L == 1)
         k_init<1><<<g, BLOCK, 0, e->s_main>>>(e->n, e->d_idx, (float*)e->d_x, (float*)e->d_r, e->nm,
-                                               ms.kind[0], 0, 0, (float)ms.beta, (float)ms.lambda);
+                                               ms.kind[0], 0, 0, (float)ms.beta, lam);
     else
         k_init<4><<<g, BLOCK, 0, e->s_main>>>(e->n, e->d_idx, (float4*)e->d_x, (float4*)e->d_r, e->nm,
-                                               ms.kind[0], ms.kind[1], ms.kind[2], (float)ms.beta, (float)ms.lambda);
+                                               ms.kind[0], ms.kind[1], ms.kind[2], (float)ms.beta, lam);
     e->launches++;
     EX_CUDA(cudaGetLastError());
     return reset_counters(e);

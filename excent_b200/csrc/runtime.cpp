@@ -41,6 +41,7 @@ struct Options {
     int device = 0;
     double budget_gb = 0;      // cap on the free device memory used for sizing (0: none)
     bool device_loop = false;  // fully cached graphs: load at setup, run the on-device pass loop
+    bool ev_init_fp64 = false; // eigenvector initial residual from the FP64 lambda1
 };
 
 static const char* USAGE =
@@ -97,6 +98,12 @@ static int parse_options(int argc, char** argv, Options& o) {
         else if (a == "--device") { if ((ok = next(v))) o.device = atoi(v); }
         else if (a == "--gpu-budget-gb") { if ((ok = next(v))) o.budget_gb = atof(v); }
         else if (a == "--device-loop") o.device_loop = true;
+        else if (a == "--ev-init") {
+            if ((ok = next(v))) {
+                if (strcmp(v, "fp64") && strcmp(v, "reference")) { fprintf(stderr, "--ev-init must be fp64 or reference\n"); return 1; }
+                o.ev_init_fp64 = !strcmp(v, "fp64");
+            }
+        }
         else { fprintf(stderr, "unknown option %s\n", a.c_str()); return 1; }
         if (!ok) return 1;
     }
@@ -127,6 +134,7 @@ static int run(const Options& o) {
         fprintf(stderr, "%s\n", excent_last_error());
         return 1;
     }
+    if (o.ev_init_fp64) M.flags |= EXCENT_EV_INIT_FP64;
     EgrFile g;
     if (g.open(o.graph.c_str(), 16, /*offsets_in_ram=*/false, true) != EXCENT_OK) {
         fprintf(stderr, "%s\n", excent_last_error());

@@ -57,7 +57,16 @@ typedef struct excent_measures {
     int divdeg[3];     /* 1: weight = scale / deg(v) (PageRank) */
     double beta;       /* Katz initial residual */
     double lambda;     /* eigenvector initial residual deg/lambda - 1 */
+    int flags;         /* EXCENT_EV_INIT_FP64 */
 } excent_measures;
+
+/* excent_measures.flags: compute the eigenvector's initial residual
+ * deg/lambda1 - 1 with the FP64 lambda1. The reference rounds lambda1 to
+ * float first (src/excent.cu:41, 372); that rounding leaves a component along
+ * the principal eigenvector in the initial residual which the push (whose
+ * operator has eigenvalue ~1 there) never removes, so on graphs with a large
+ * (v1 . 1) the hub residuals can stay above a small eps for good. */
+#define EXCENT_EV_INIT_FP64 1
 
 /* Build the table for --measure pr|katz|ev|all with the reference's
  * validation and float rounding (src/excent.cu:307-316, 344-351). Negative
@@ -318,6 +327,44 @@ int excent_batch_stats(excent_batch* b, int* passes, unsigned long long* pushed_
 int excent_batch_read(excent_batch* b, int lane, int residual, float* out);
 int excent_batch_stream(excent_batch* b, void** stream);
 int excent_batch_launches(excent_batch* b, unsigned long long* launches);
+
+/* ------------------------------------------------------------ adjoint (VJP) */
+
+/* A weighted directed graph on the device: forward CSR (out-lists) and raw
+ * float32 weights given as device pointers (kept by the caller), row-normalised
+ * weights wn = w / rowsum, and a transposed CSR with the edge permutation.
+ * Forward fixed points: PageRank x = (1 - d) t + d W^T x (t: a teleport
+ * vector, NULL = all ones) and Katz x = beta + alpha W^T x, solved by a
+ * weighted delta-push to an absolute eps. The VJP of a scalar loss with
+ * dL/dx = c solves lambda = c + s W lambda by the same push on the transposed
+ * lists and returns dL/dt (or dL/dbeta) and dL/dw for the raw weights through
+ * the normalisation. All vectors are device pointers. No reference
+ * counterpart: the reference has neither weights nor gradients. */
+typedef struct excent_wgraph excent_wgraph;
+int excent_wgraph_create(int device, int n, unsigned long long m, const unsigned long long* d_idx, const int32_t* d_adj,
+                         const float* d_w, excent_wgraph** out);
+int excent_wgraph_destroy(excent_wgraph* g);
+/* New raw weights (device pointer, CSR order): renormalise. */
+int excent_wgraph_set_weights(excent_wgraph* g, const float* d_w);
+/* kind EXCENT_PR (s = d) or EXCENT_KATZ (s = alpha); d_t: teleport / beta
+ * (n floats, NULL = ones); result copied to d_x_out when not NULL and kept
+ * for the VJP. */
+int excent_wgraph_forward(excent_wgraph* g, int kind, double s, const float* d_t, float eps, int max_passes,
+                          float* d_x_out, int* passes, unsigned long long* pushed);
+/* Adjoint solve for dL/dx = d_c after excent_wgraph_forward; writes dL/dt
+ * (n) and dL/dw (m, CSR order of the forward graph) where not NULL. */
+int excent_wgraph_vjp(excent_wgraph* g, const float* d_c, float eps, int max_passes, float* d_grad_t, float* d_grad_w,
+                      int* passes, unsigned long long* pushed);
+/* The adjoint vector lambda of the last VJP (n floats, device). */
+int excent_wgraph_lambda(excent_wgraph* g, float* d_out);
+/* FP64 Jacobi checks: loss c . x with raw weight `edge` shifted by delta
+ * (edge < 0: none), and the FP64 gradient (dL/dt into grad_t[n], dL/dw into
+ * grad_w[m], host arrays, either may be NULL). */
+int excent_wgraph_loss_fp64(excent_wgraph* g, int kind, double s, const float* d_t, const float* d_c, long long edge,
+                            double delta, double tol, double* loss);
+int excent_wgraph_grad_fp64(excent_wgraph* g, int kind, double s, const float* d_t, const float* d_c, double tol,
+                            double* grad_t, double* grad_w);
+int excent_wgraph_stream(excent_wgraph* g, void** stream);
 
 /* ------------------------------------------------------------ FP64 tools */
 
