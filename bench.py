@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--scale", type=int, default=None, help="override the graph scale (smaller test runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="host-driven pass loop instead of the CUDA graph")
+    ap.add_argument("--ev-project", default="on", choices=["on", "off"],
+                    help="FP64 eigenvector normalisation step (remove the principal-eigenvector component of the "
+                         "eigenvector residual each pass); the `all` run does not reach eps 1e-6 at scale 24 without it")
     ap.add_argument("--ev-init", default="fp64", choices=["fp64", "reference"],
                     help="eigenvector initial residual from the FP64 lambda1 (default) or from lambda1 rounded to "
                          "float as the reference does")
@@ -144,8 +147,10 @@ def run_ours(a, world, rank, local, dist):
     n, m = g.n, g.m
     d_idx, d_adj, _ = g.device_ptrs()
     log(f"graph scale {scale}: n={n} m={m}")
+    v1 = None
     if measure == "all":
-        par = X.params_fp64(n, d_idx, d_adj, device=local)
+        v1 = torch.empty(n, dtype=torch.float32, device="cuda")
+        par = X.params_fp64(n, d_idx, d_adj, device=local, v1_out=v1)
         lam = par["lambda"]
         log(f"lambda1 {lam:.6f} after {par['sweeps']} sweeps")
         meas = X.measures("all", alpha=0.9 / lam, beta=1.0, lam=lam, eps_pr=1e-2, eps_katz=1e-6, eps_ev=1e-6,
@@ -162,6 +167,8 @@ def run_ours(a, world, rank, local, dist):
     v0, e = X.plan_chunks(idx_np, X.chunk_cap(m))
     eng = X.Engine(n, m, meas, v0, e, device=local)
     eng.upload_device(d_idx, d_adj)
+    if v1 is not None and a.ev_project == "on":
+        eng.ev_project(v1)
     use_graph = not a.no_graph
     for _ in range(a.warmup):
         s = eng.solve(use_graph=use_graph)
@@ -259,7 +266,7 @@ def run_ours(a, world, rank, local, dist):
                    "pushed_per_solve": int(pushed / a.steps), "time_to_eps_ms": round(t / a.steps * 1e3, 3),
                    "l2_note": "inputs larger than L2 (edge cache %.2f GB)" % (m * 4 / 1e9),
                    "cuda_graph": use_graph, "parallelism": f"{world} independent replicas",
-                   "ev_init": a.ev_init},
+                   "ev_init": a.ev_init, "ev_project": a.ev_project if measure == "all" else None},
         "e2e": {"value": round(e_pushed / te / 1e9, 4), "unit": "GTEPS", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": round(te / a.steps * 1e3, 3),
                 "wall_ms_per_step": round(te_wall / a.steps * 1e3, 3)},

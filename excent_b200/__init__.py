@@ -201,6 +201,10 @@ class Engine:
     def results(self):
         return [self.read(i) for i in range(self.meas.nm)]
 
+    def ev_project(self, v1):
+        """FP64 eigenvector normalisation step with the unit principal eigenvector v1 (None: off)."""
+        call("excent_engine_ev_project", self.h, _ptr(v1))
+
     def stream(self):
         """The engine's cudaStream_t as an integer handle (torch.cuda.ExternalStream accepts it)."""
         s = C.c_void_p()
@@ -218,12 +222,13 @@ class Engine:
         return dict(zip(("snapshot", "plan", "push", "hub"), ms.tolist())), p.value
 
 
-def params_fp64(n, d_idx, d_adj, katz_numerator=0.85, device=0):
+def params_fp64(n, d_idx, d_adj, katz_numerator=0.85, device=0, v1_out=None):
     """Given constants of a device-resident symmetric graph (tools/excent_params.cu:133-163):
-    {lambda, alpha, mean_ev, mean_katz, sweeps}."""
+    {lambda, alpha, mean_ev, mean_katz, sweeps}; v1_out (device buffer of n float32) receives
+    the unit principal eigenvector."""
     out = np.zeros(5, dtype=np.float64)
     call("excent_params_fp64", int(device), int(n), _ptr(d_idx), _ptr(d_adj), float(katz_numerator),
-         _tp(out, _capi.f64p))
+         _tp(out, _capi.f64p), _ptr(v1_out))
     return {"lambda": out[0], "alpha": out[1], "mean_ev": out[2], "mean_katz": out[3], "sweeps": int(out[4])}
 
 

@@ -96,7 +96,8 @@ PROTOS = [
                                           f64p]),
     ("excent_wgraph_grad_fp64", C.c_int, [vp, C.c_int, C.c_double, vp, vp, C.c_double, vp, vp]),
     ("excent_wgraph_stream", C.c_int, [vp, C.POINTER(vp)]),
-    ("excent_params_fp64", C.c_int, [C.c_int, C.c_int, vp, vp, C.c_double, f64p]),
+    ("excent_params_fp64", C.c_int, [C.c_int, C.c_int, vp, vp, C.c_double, f64p, vp]),
+    ("excent_engine_ev_project", C.c_int, [vp, vp]),
     ("excent_reference_fp64", C.c_int, [C.c_int, C.c_int, vp, vp, C.c_int, C.c_double, C.c_double, C.c_double,
                                         C.c_int, f64p, C.POINTER(C.c_int)]),
     ("excent_device_info", C.c_int, [C.c_int, vp]),

@@ -122,10 +122,13 @@ __device__ __forceinline__ void warp_scatter(P* r, const int* nb, unsigned deg, 
     const int4* body = reinterpret_cast<const int4*>(nb + head);
     const unsigned nbody = (deg - head) >> 2;
     unsigned i = lane;
-    for (; i + 32 < nbody; i += 64) {
+    for (; i + 96 < nbody; i += 128) {  // four 128-bit loads in flight per lane
         const int4 q0 = ld_edge4(body + i), q1 = ld_edge4(body + i + 32);
+        const int4 q2 = ld_edge4(body + i + 64), q3 = ld_edge4(body + i + 96);
         red_add(r, q0.x, p); red_add(r, q0.y, p); red_add(r, q0.z, p); red_add(r, q0.w, p);
         red_add(r, q1.x, p); red_add(r, q1.y, p); red_add(r, q1.z, p); red_add(r, q1.w, p);
+        red_add(r, q2.x, p); red_add(r, q2.y, p); red_add(r, q2.z, p); red_add(r, q2.w, p);
+        red_add(r, q3.x, p); red_add(r, q3.y, p); red_add(r, q3.z, p); red_add(r, q3.w, p);
     }
     for (; i < nbody; i += 32) {
         const int4 q = ld_edge4(body + i);

@@ -21,9 +21,9 @@
 namespace excent {
 
 static constexpr int SNAP_GROUP = 16;     // bitmap words per warp step in the snapshot (512 vertices)
-static constexpr unsigned SMALL_MAX = 32; // degree <= 32: edge-balanced across the warp
-static constexpr unsigned HUB_MIN = 2048; // degree > 2048: split into segments for whole warps
-static constexpr unsigned HUB_SEG = 2048; // edges per hub segment
+static constexpr unsigned HUB_MIN = 256;  // degree > 256: split into segments for whole warps
+static constexpr unsigned HUB_SEG = 1024; // edges per hub segment
+static constexpr int UNROLL = 4;          // independent index loads per lane in flight
 static constexpr int BLOCK = 256;
 
 enum { SRC_TABLE = 0, SRC_CHUNK = 1, SRC_GATHER = 2, SRC_HOT = 3 };
@@ -49,6 +49,8 @@ struct Ctrl {
     double rsum[MAXM]; // FP64 sum |r| of the last snapshot
     unsigned hcount;   // hot pending list length
     unsigned pad2;
+    double ev_dot;     // FP64 (r_ev . v1) accumulated by the snapshot
+    double ev_corr;    // component removed from r_ev by the next snapshot
 };
 
 struct PassRec {
@@ -59,7 +61,9 @@ struct PassRec {
 
 struct SnapArgs {
     int n, nc, words, groups_per_warp;
-    const void* r;
+    void* r;
+    const float* v1;   // unit principal eigenvector (EV normalisation step) or null
+    int ev;            // measure index of the eigenvector
     DevMeasures M;
     const ull* idx;
     const int* cv0;
@@ -148,13 +152,14 @@ __device__ __forceinline__ int chunk_of(long long v, const int* cv0, int nc) {
 template <int L>
 __global__ void __launch_bounds__(BLOCK) k_snapshot(SnapArgs a) {
     typedef typename Lane<L>::T T;
-    const T* r = reinterpret_cast<const T*>(a.r);
+    T* r = reinterpret_cast<T*>(a.r);
     const int lane = threadIdx.x & 31;
     const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long ngroups = (a.words + SNAP_GROUP - 1) / SNAP_GROUP;
     long long g0 = gw * a.groups_per_warp, g1 = g0 + a.groups_per_warp;
     if (g1 > ngroups) g1 = ngroups;
-    double rs0 = 0, rs1 = 0, rs2 = 0;
+    double rs0 = 0, rs1 = 0, rs2 = 0, evd = 0;
+    const double evc = a.v1 ? a.ctrl->ev_corr : 0.0;
     unsigned hp = 0;
     for (long long g = g0; g < g1; g++) {
         const long long w0 = g * SNAP_GROUP;
@@ -167,7 +172,21 @@ __global__ void __launch_bounds__(BLOCK) k_snapshot(SnapArgs a) {
             const long long v = (w0 + j) * 32 + lane;
             bool pend = false;
             if (v < a.n) {
-                const T rv = r[v];
+                T rv = r[v];
+                if (a.v1) {  // FP64 normalisation: drop the v1 component the push cannot remove
+                    const float q = a.v1[v];
+                    float* rp = reinterpret_cast<float*>(r + v) + (L == 1 ? 0 : a.ev);
+                    float re;
+                    if constexpr (L == 4) re = a.ev == 0 ? rv.x : a.ev == 1 ? rv.y : rv.z;
+                    else re = rv;
+                    if (evc != 0.0) {
+                        re = (float)((double)re - evc * (double)q);
+                        *rp = re;
+                        if constexpr (L == 4) { if (a.ev == 0) rv.x = re; else if (a.ev == 1) rv.y = re; else rv.z = re; }
+                        else rv = re;
+                    }
+                    evd += (double)re * (double)q;
+                }
                 if constexpr (L == 1) rs0 += fabs((double)rv);
                 else {
                     rs0 += fabs((double)rv.x);
@@ -234,17 +253,19 @@ __global__ void __launch_bounds__(BLOCK) k_snapshot(SnapArgs a) {
         }
     }
     // FP64 termination residual and hot pending count: block reduction, one atomic each
-    __shared__ double s_rs[3][BLOCK / 32];
+    __shared__ double s_rs[4][BLOCK / 32];
     __shared__ unsigned s_hp[BLOCK / 32];
     rs0 = warp_sum(rs0); rs1 = warp_sum(rs1); rs2 = warp_sum(rs2);
+    evd = warp_sum(evd);
     hp = warp_sum(hp);
     const int wib = threadIdx.x >> 5;
-    if (lane == 0) { s_rs[0][wib] = rs0; s_rs[1][wib] = rs1; s_rs[2][wib] = rs2; s_hp[wib] = hp; }
+    if (lane == 0) { s_rs[0][wib] = rs0; s_rs[1][wib] = rs1; s_rs[2][wib] = rs2; s_rs[3][wib] = evd; s_hp[wib] = hp; }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double t0 = 0, t1 = 0, t2 = 0;
+        double t0 = 0, t1 = 0, t2 = 0, t3 = 0;
         unsigned th = 0;
-        for (int i = 0; i < BLOCK / 32; i++) { t0 += s_rs[0][i]; t1 += s_rs[1][i]; t2 += s_rs[2][i]; th += s_hp[i]; }
+        for (int i = 0; i < BLOCK / 32; i++) { t0 += s_rs[0][i]; t1 += s_rs[1][i]; t2 += s_rs[2][i]; t3 += s_rs[3][i]; th += s_hp[i]; }
+        if (a.v1) atomicAdd(&a.ctrl->ev_dot, t3);
         atomicAdd(&a.ctrl->rsum[0], t0);
         if (a.M.nm > 1) atomicAdd(&a.ctrl->rsum[1], t1);
         if (a.M.nm > 2) atomicAdd(&a.ctrl->rsum[2], t2);
@@ -311,6 +332,8 @@ __global__ void k_plan(int nc, const int* cv0, int n, ull* cnt, const uint8_t* c
         if (stop) ctrl->done = 1; else ctrl->pass = p + 1;
         *hub_cnt = 0;
         ctrl->hotpend = 0;
+        ctrl->ev_corr = ctrl->ev_dot;
+        ctrl->ev_dot = 0;
         if (!stop) for (int k = 0; k < MAXM; k++) ctrl->rsum[k] = 0;
         if (use_cond) cudaGraphSetConditional(cond, stop ? 0u : 1u);
     }
@@ -408,8 +431,6 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
             act = nonzero(p) && deg > 0;
         }
         if (act) pushed += deg;
-        const bool small = act && deg <= SMALL_MAX;
-        const bool medium = act && deg > SMALL_MAX && deg <= HUB_MIN;
         const bool large = act && deg > HUB_MIN;
         if (large) {
             const unsigned nseg = (unsigned)((deg + HUB_SEG - 1) / HUB_SEG);
@@ -428,35 +449,35 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
                 atomicExch(&a.ctrl->err, 1);
             }
         }
-        uint32_t mm = __ballot_sync(FULL, medium);
-        while (mm) {
-            const int sl = __ffs(mm) - 1;
-            mm &= mm - 1;
-            const int* nbm = shfl_ptr(nb, sl);
-            const unsigned dm = __shfl_sync(FULL, (unsigned)deg, sl);
-            const T pm = shfl(p, sl);
-            warp_scatter(r, nbm, dm, pm, lane);
-        }
-        const unsigned ds = small ? (unsigned)deg : 0u;
+        // every other list of the tile, edge-balanced: the tile's lists are
+        // concatenated and lane j handles entry j of each 32-entry slice, UNROLL
+        // slices at a time so each lane has UNROLL index loads in flight
+        const unsigned ds = (act && !large) ? (unsigned)deg : 0u;
         const unsigned incl = warp_incl_scan(ds, lane);
         const unsigned tot = __shfl_sync(FULL, incl, 31);
         if (tot) {
             s_nb[wib][lane] = nb;
             s_ex[wib][lane] = incl - ds;
-            if (small) s_p[wib][lane] = p;
+            if (ds) s_p[wib][lane] = p;
             __syncwarp();
-            for (unsigned j0 = 0; j0 < tot; j0 += 32) {
-                const unsigned j = j0 + lane;
-                int lo = 0;
+            for (unsigned j0 = 0; j0 < tot; j0 += 32 * UNROLL) {
+                int u[UNROLL];
+                int own[UNROLL];
 #pragma unroll
-                for (int step = 16; step > 0; step >>= 1) {
-                    const unsigned val = __shfl_sync(FULL, incl, lo + step - 1);
-                    if (val <= j) lo += step;
+                for (int k = 0; k < UNROLL; k++) {
+                    const unsigned j = j0 + 32 * k + lane;
+                    int lo = 0;
+#pragma unroll
+                    for (int step = 16; step > 0; step >>= 1) {
+                        const unsigned val = __shfl_sync(FULL, incl, lo + step - 1);
+                        if (val <= j) lo += step;
+                    }
+                    own[k] = j < tot ? lo : -1;
+                    u[k] = j < tot ? ld_edge(s_nb[wib][lo] + (j - s_ex[wib][lo])) : 0;
                 }
-                if (j < tot) {
-                    const int u = ld_edge(s_nb[wib][lo] + (j - s_ex[wib][lo]));
-                    red_add(r, u, s_p[wib][lo]);
-                }
+#pragma unroll
+                for (int k = 0; k < UNROLL; k++)
+                    if (own[k] >= 0) red_add(r, u[k], s_p[wib][own[k]]);
             }
             __syncwarp();
         }
@@ -588,6 +609,9 @@ struct excent_engine {
     uint16_t* d_trace = nullptr;
     bool trace_on = false;
     float* d_tmp = nullptr;  // n floats for readback of the float4 layout
+    float* d_v1 = nullptr;   // unit principal eigenvector for the EV normalisation step
+    bool ev_proj = false;
+    int ev_index = -1;
     int* d_cache = nullptr;
     ull cache_edges = 0;
     // hot cache
@@ -634,7 +658,7 @@ static int free_engine(excent_engine* e) {
     cudaDeviceSynchronize();
     if (e->gexec) cudaGraphExecDestroy(e->gexec);
     if (e->graph) cudaGraphDestroy(e->graph);
-    void* dptrs[] = {e->d_idx, e->d_x, e->d_r, e->d_bitmap, e->d_cnt, e->d_cv0, e->d_list, e->d_ctrl, e->d_cmode,
+    void* dptrs[] = {e->d_v1, e->d_idx, e->d_x, e->d_r, e->d_bitmap, e->d_cnt, e->d_cv0, e->d_list, e->d_ctrl, e->d_cmode,
                      e->d_wt_type, e->d_wt_prefix, e->d_hubq[0], e->d_hubq[1], e->d_hubq[2], e->d_hubcnt, e->d_log, e->d_trace, e->d_tmp, e->d_cache,
                      e->d_hids, e->d_hoff, e->d_hedges, e->d_hot, e->d_hlist};
     for (void* p : dptrs) if (p) cudaFree(p);
@@ -702,7 +726,7 @@ static int engine_setup(excent_engine* e, int device, int n, ull m, const excent
     EX_ALLOC(e->d_cmode, (size_t)nc);
     EX_ALLOC(e->d_wt_type, (size_t)nc);
     EX_ALLOC(e->d_wt_prefix, ((size_t)nc + 1) * sizeof(unsigned));
-    e->hub_cap[0] = 2 * (m / HUB_SEG) + 64;
+    e->hub_cap[0] = m / HUB_SEG + m / HUB_MIN + 64;
     EX_ALLOC(e->d_hubq[0], e->hub_cap[0] * sizeof(HubSeg));
     EX_ALLOC(e->d_hubcnt, 3 * sizeof(ull));
     e->log_cap = 1 << 17;
@@ -894,6 +918,8 @@ static SnapArgs snap_args(excent_engine* e, bool use_hot) {
     SnapArgs a{};
     a.n = e->n; a.nc = e->nc; a.words = (int)(((size_t)e->n + 31) / 32); a.groups_per_warp = e->groups_per_warp;
     a.r = e->d_r; a.M = e->M; a.idx = e->d_idx; a.cv0 = e->d_cv0;
+    a.v1 = e->ev_proj ? e->d_v1 : nullptr;
+    a.ev = e->ev_index;
     a.hot = use_hot ? e->d_hot : nullptr;
     a.bitmap = e->d_bitmap; a.cnt = e->d_cnt; a.list = e->d_list;
     a.trace = e->trace_on ? e->d_trace : nullptr;
@@ -922,6 +948,13 @@ extern "C" int excent_engine_snapshot(excent_engine* e, int use_hot, unsigned lo
     EX_CUDA(cudaMemcpyAsync(e->h_cnt, e->d_cnt, 2 * (size_t)e->nc * sizeof(ull), cudaMemcpyDeviceToHost, e->s_main));
     EX_CUDA(cudaMemcpyAsync(e->h_ctrl, e->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, e->s_main));
     EX_CUDA(cudaStreamSynchronize(e->s_main));
+    if (e->ev_proj) {   // next snapshot removes the component measured by this one
+        Ctrl* hc = e->h_ctrl;
+        hc->ev_corr = hc->ev_dot;
+        hc->ev_dot = 0;
+        EX_CUDA(cudaMemcpyAsync(&e->d_ctrl->ev_dot, &hc->ev_dot, 2 * sizeof(double), cudaMemcpyHostToDevice, e->s_main));
+        EX_CUDA(cudaStreamSynchronize(e->s_main));
+    }
     if (cnt) memcpy(cnt, e->h_cnt, 2 * (size_t)e->nc * sizeof(ull));
     if (hotpend) *hotpend = e->h_ctrl->hotpend;
     if (rsum) for (int k = 0; k < e->nm; k++) rsum[k] = e->h_ctrl->rsum[k];
@@ -1038,7 +1071,8 @@ extern "C" int excent_engine_slots_create(excent_engine* e, unsigned long long m
         EX_CUDA(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
     }
     for (int q = 1; q < 3; q++) {
-        e->hub_cap[q] = 2 * (std::max<ull>(max_chunk_edges, 1) / HUB_SEG) + 64;
+        const ull me = std::max<ull>(max_chunk_edges, 1);
+        e->hub_cap[q] = me / HUB_SEG + me / HUB_MIN + 64;
         EX_ALLOC(e->d_hubq[q], e->hub_cap[q] * sizeof(HubSeg));
     }
     e->max_chunk_edges = std::max<ull>(e->max_chunk_edges, max_chunk_edges);
@@ -1388,6 +1422,21 @@ extern "C" int excent_device_info(int device, excent_device_info_t* out) {
     EX_CUDA(cudaDeviceGetAttribute(&out->sms, cudaDevAttrMultiProcessorCount, device));
     EX_CUDA(cudaDeviceGetAttribute(&out->cc_major, cudaDevAttrComputeCapabilityMajor, device));
     EX_CUDA(cudaDeviceGetAttribute(&out->cc_minor, cudaDevAttrComputeCapabilityMinor, device));
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_ev_project(excent_engine* e, const float* d_v1) {
+    EX_CHECK_ARG(e, "null engine");
+    EX_CUDA(cudaSetDevice(e->dev));
+    invalidate_graph(e);
+    if (!d_v1) { e->ev_proj = false; return EXCENT_OK; }
+    int ev = -1;
+    for (int i = 0; i < e->nm; i++) if (e->meas.kind[i] == EXCENT_EV) ev = i;
+    EX_CHECK_ARG(ev >= 0, "the run has no eigenvector measure");
+    if (!e->d_v1) EX_ALLOC(e->d_v1, (size_t)e->n * sizeof(float));
+    EX_CUDA(cudaMemcpy(e->d_v1, d_v1, (size_t)e->n * sizeof(float), cudaMemcpyDefault));
+    e->ev_index = ev;
+    e->ev_proj = true;
     return EXCENT_OK;
 }
 

@@ -95,8 +95,13 @@ int norms(int n, const double* x, const double* y, Bufs& B, int grid, double* ss
 }
 }  // namespace
 
+__global__ void k_tofloat(int n, const double* x, float* y) {
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x)
+        y[v] = (float)x[v];
+}
+
 extern "C" int excent_params_fp64(int device, int n, const unsigned long long* d_idx, const int32_t* d_adj,
-                                  double katz_numerator, double* out) {
+                                  double katz_numerator, double* out, float* d_v1) {
     EX_CHECK_ARG(n >= 1 && d_idx && d_adj && out, "bad argument");
     EX_CUDA(cudaSetDevice(device));
     int sms = 0;
@@ -123,6 +128,7 @@ extern "C" int excent_params_fp64(int device, int n, const unsigned long long* d
     }
     EX_TRY(norms(n, B.v[0], nullptr, B, G, nullptr, &vsum, nullptr));
     const double meanEV = vsum * vsum / n;
+    if (d_v1) k_tofloat<<<G, 256>>>(n, B.v[0], d_v1);  // unit principal eigenvector
     // Katz fixed point x = 1 + alpha A x, alpha = katz_numerator / lambda1, for its mean (:150-162)
     const double alpha = katz_numerator / lam;
     k_scale64<<<G, 256>>>(n, B.v[0], 0.0, 1.0);

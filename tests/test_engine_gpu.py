@@ -265,3 +265,27 @@ def test_error_no_looser_than_reference_engine(sample, measure):
         assert ours["max_abs"] <= theirs["max_abs"] * 1.10, (k, ours, theirs)
         assert ours["top1000"] >= theirs["top1000"] - 3
     eng.close()
+
+
+def test_ev_normalisation_step_keeps_the_unit_eigenvector(rmat16):
+    """EV with the FP64 normalisation step converges to the same unit vector
+    (checked against the FP64 oracle) at a tight eps."""
+    n, idx, adj = rmat16
+    dev = torch.device("cuda")
+    d_idx = torch.from_numpy(idx.view(np.int64)).to(dev)
+    d_adj = torch.from_numpy(adj).to(dev)
+    v1 = torch.empty(n, dtype=torch.float32, device=dev)
+    par = X.params_fp64(n, d_idx.data_ptr(), d_adj.data_ptr(), v1_out=v1)
+    ref = O.reference_solution(n, idx, adj, "ev")
+    assert np.abs(O.unit(v1.cpu().numpy()) - O.unit(ref)).max() < 1e-5
+    for proj in (False, True):
+        meas = X.measures("ev", lam=par["lambda"], eps_ev=1e-6)
+        eng = make_engine(n, idx, adj, meas)
+        if proj:
+            eng.ev_project(v1)
+        st = eng.solve(max_passes=5000)
+        c = O.compare("ev", ref, eng.read(0))
+        print("projection", proj, "passes", st.passes, c)
+        assert st.passes < 5000
+        assert c["l1_rel"] < 2e-3 and c["top1000"] >= 990
+        eng.close()
