@@ -1,0 +1,139 @@
+"""The excent command line end to end on a GPU, in every fetch mode (HBM
+chunk cache, streamed chunks, gathered lists, high-degree cache, zero copy),
+against the FP64 oracle and against the reference binary built from source
+(oracle/_ref/excent) on the same graph and flags."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import GOLDEN, read_env
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("needs a GPU", allow_module_level=True)
+
+import excent_b200._capi as K  # noqa: E402
+
+CLI = K.CLI_PATH
+REF_CLI = os.path.join(O.REF_DIR, "excent")
+SAMPLE = os.path.join(GOLDEN, "sample.egr")
+
+
+def env_args(env, measure):
+    a = ["--measure", measure]
+    if measure in ("katz", "all"):
+        a += ["--alpha", env["ALPHA"], "--beta", env["BETA"], "--eps-katz", env["EPS_KATZ"]]
+    if measure in ("ev", "all"):
+        a += ["--lambda", env["LAMBDA"], "--eps-ev", env["EPS_EV"]]
+    return a
+
+
+def run(binary, args, tmp):
+    e = dict(os.environ, HOME=str(tmp))
+    r = subprocess.run([binary, *args], capture_output=True, text=True, env=e, timeout=600)
+    assert r.returncode == 0, r.stderr + r.stdout
+    return r.stdout
+
+
+@pytest.fixture(scope="module")
+def rmat14(tmp_path_factory):
+    d = tmp_path_factory.mktemp("cli")
+    n, idx, adj = O.rmat_graph(14, 16, 5)
+    p = str(d / "r14.egr")
+    O.write_egr(p, idx, adj, wide=True)
+    par = O.params(n, idx, adj)
+    env = {k: par[k] for k in ("LAMBDA", "ALPHA", "BETA", "EPS_PR", "EPS_KATZ", "EPS_EV")}
+    return p, n, idx, adj, env
+
+
+MODES = {
+    "cached": ["--stream-ratio", "2", "--cache", "chunks"],
+    "stream": ["--stream-ratio", "0", "--cache", "none"],
+    "gather": ["--stream-ratio", "2", "--cache", "none"],
+    "mixed": ["--stream-ratio", "0.3", "--cache", "none", "--chunk-medges", "0.02"],
+    "hot": ["--stream-ratio", "0.3", "--cache", "hot", "--chunk-medges", "0.02", "--gpu-budget-gb", "0.0012",
+            "--reserve-mb", "0"],
+    "hot-start": ["--stream-ratio", "2", "--cache", "hot", "--hot-when", "both", "--hot-order", "ranges",
+                  "--chunk-medges", "0.02", "--gpu-budget-gb", "0.0012", "--reserve-mb", "0"],
+    "zero-copy": ["--stream-ratio", "0.3", "--cache", "none", "--zero-copy", "on", "--chunk-medges", "0.02"],
+    "device-loop": ["--stream-ratio", "2", "--cache", "chunks", "--device-loop"],
+    "nodedup": ["--stream-ratio", "2", "--cache", "none", "--dedup", "off", "--chunk-medges", "0.05"],
+}
+
+
+@pytest.mark.parametrize("mode", sorted(MODES))
+@pytest.mark.parametrize("measure", ["pr", "all"])
+def test_cli_modes_vs_oracle(rmat14, tmp_path, mode, measure):
+    p, n, idx, adj, env = rmat14
+    out = run(CLI, [p, *env_args(env, measure), *MODES[mode], "--dump", str(tmp_path / "o"), "--count-pushes"],
+              tmp_path)
+    assert re.search(r"^passes \d+  measure", out, re.M), out
+    if mode in ("stream", "mixed", "zero-copy"):
+        assert re.search(r"stream [1-9]", out), out
+    if mode in ("gather", "mixed", "nodedup"):
+        assert re.search(r"gather [1-9]", out), out
+    if mode.startswith("hot"):
+        assert "GPU degree cache:" in out
+        assert re.search(r"cached high-degree pending [1-9]", out), out
+    names = ["pr", "katz", "ev"] if measure == "all" else ["pr"]
+    for k in names:
+        x = np.fromfile(str(tmp_path / f"o.{k}.bin"), dtype=np.float32)
+        ref = O.reference_solution(n, idx, adj, k, alpha=float(env["ALPHA"]))
+        c = O.compare(k, ref, x)
+        assert c["l1_rel"] < 0.05 and c["top100"] >= 95, (mode, k, c)
+
+
+def test_cli_sample_matches_reference_binary(tmp_path):
+    if not os.path.exists(REF_CLI):
+        pytest.skip("reference binary not built")
+    env = read_env(os.path.join(GOLDEN, "sample.env"))
+    for measure in ("pr", "all"):
+        args = [SAMPLE, *env_args(env, measure), "--stream-ratio", "2"]
+        ours = run(CLI, args + ["--dump", str(tmp_path / "a")], tmp_path)
+        ref = run(REF_CLI, args + ["--dump", str(tmp_path / "b")], tmp_path)
+        # same line structure (first words of every line)
+        heads = lambda s: [re.sub(r"[-0-9.e+]+", "#", l)[:25] for l in s.splitlines() if not l.startswith("throughput")]  # noqa: E731
+        h1, h2 = heads(ours), heads(ref)
+        assert h1[:4] == h2[:4]
+        assert [l for l in h1 if l.startswith("passes")] and [l for l in h2 if l.startswith("passes")]
+        names = ["pr", "katz", "ev"] if measure == "all" else ["pr"]
+        for k in names:
+            a = np.fromfile(str(tmp_path / f"a.{k}.bin"), dtype=np.float32)
+            b = np.fromfile(str(tmp_path / f"b.{k}.bin"), dtype=np.float32)
+            ref_x = O.reference_solution(len(a), *O.read_egr(SAMPLE)[1:], k, alpha=float(env["ALPHA"]))
+            ca, cb = O.compare(k, ref_x, a), O.compare(k, ref_x, b)
+            assert ca["l1_rel"] <= cb["l1_rel"] * 1.05, (k, ca, cb)
+
+
+def test_cli_trace_and_hot_rank_roundtrip(rmat14, tmp_path):
+    """--trace-pending writes uint16 pass counts; they drive --hot-rank."""
+    p, n, idx, adj, env = rmat14
+    tr = str(tmp_path / "trace.u16")
+    run(CLI, [p, "--measure", "pr", "--stream-ratio", "2", "--trace-pending", tr], tmp_path)
+    t = np.fromfile(tr, dtype=np.uint16)
+    assert len(t) == n and t.max() > 0
+    out = run(CLI, [p, "--measure", "pr", "--stream-ratio", "0.3", "--cache", "hot", "--hot-rank", tr,
+                    "--chunk-medges", "0.02", "--gpu-budget-gb", "0.0012", "--reserve-mb", "0",
+                    "--dump", str(tmp_path / "h")], tmp_path)
+    assert "GPU cache ranked by passes pending" in out
+    x = np.fromfile(str(tmp_path / "h.pr.bin"), dtype=np.float32)
+    ref = O.reference_solution(n, idx, adj, "pr")
+    assert O.compare("pr", ref, x)["l1_rel"] < 0.05
+
+
+def test_cli_tau_calibration_and_cache_file(rmat14, tmp_path):
+    p, *_ = rmat14
+    out = run(CLI, [p, "--measure", "pr", "--cache", "none"], tmp_path)
+    m = re.search(r"fetch rule: tau = ([0-9.]+) \(stream", out)
+    assert m, out
+    files = list((tmp_path / ".cache" / "excent").glob("*.tau"))
+    assert len(files) == 1
+    tau, t = open(files[0]).read().split()
+    assert abs(float(tau) - float(m.group(1))) < 1e-3
+    out2 = run(CLI, [p, "--measure", "pr", "--cache", "none"], tmp_path)
+    assert "measured earlier on this machine" in out2
