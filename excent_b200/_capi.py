@@ -76,6 +76,8 @@ PROTOS = [
     ("excent_batch_read", C.c_int, [vp, C.c_int, C.c_int, vp]),
     ("excent_batch_stream", C.c_int, [vp, C.POINTER(vp)]),
     ("excent_batch_launches", C.c_int, [vp, u64p]),
+    ("excent_batch_autotune", C.c_int, [C.c_int, C.c_int, u64, vp, vp, C.c_int, C.c_double, C.c_int, vp, vp, vp, vp,
+                                        C.c_int, C.POINTER(C.c_int), f64p]),
     ("excent_engine_stats", C.c_int, [vp, C.POINTER(Stats), C.POINTER(PassLog), C.c_int]),
     ("excent_engine_read", C.c_int, [vp, C.c_int, C.c_int, vp, u64, u64]),
     ("excent_engine_write", C.c_int, [vp, C.c_int, vp, vp]),
@@ -98,6 +100,7 @@ PROTOS = [
     ("excent_wgraph_stream", C.c_int, [vp, C.POINTER(vp)]),
     ("excent_params_fp64", C.c_int, [C.c_int, C.c_int, vp, vp, C.c_double, f64p, vp]),
     ("excent_engine_ev_project", C.c_int, [vp, vp]),
+    ("excent_params_fp64_noalloc", C.c_int, [C.c_int, C.c_int, vp, vp, C.c_double, f64p, vp]),
     ("excent_reference_fp64", C.c_int, [C.c_int, C.c_int, vp, vp, C.c_int, C.c_double, C.c_double, C.c_double,
                                         C.c_int, f64p, C.POINTER(C.c_int)]),
     ("excent_device_info", C.c_int, [C.c_int, vp]),

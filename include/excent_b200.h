@@ -336,6 +336,12 @@ int excent_batch_stats(excent_batch* b, int* passes, unsigned long long* pushed_
 /* Values (or residuals) of lane q for all n vertices, to host float32. */
 int excent_batch_read(excent_batch* b, int lane, int residual, float* out);
 int excent_batch_stream(excent_batch* b, void** stream);
+/* Autotuner: time one batch of min(B, nq) of the given queries (seeded as
+ * in excent_batch_seed) at each width B in {32, 64, 128, 256} and return the
+ * width with the lowest time per query; per_query_ms[4] gets the times. */
+int excent_batch_autotune(int device, int n, unsigned long long m, const unsigned long long* d_idx, const int32_t* d_adj,
+                          int kind, double d_or_alpha, int nq, const int* lane_off, const int32_t* vids,
+                          const float* vals, const float* eps, int max_passes, int* best_B, double* per_query_ms);
 int excent_batch_launches(excent_batch* b, unsigned long long* launches);
 
 /* ------------------------------------------------------------ adjoint (VJP) */
@@ -387,6 +393,20 @@ int excent_wgraph_stream(excent_wgraph* g, void** stream);
  * may be NULL) receives the unit principal eigenvector. tools/excent_params.cu:133-163. */
 int excent_params_fp64(int device, int n, const unsigned long long* d_idx, const int32_t* d_adj,
                        double katz_numerator, double* out, float* d_v1);
+/* Same results as excent_params_fp64, but the call allocates no device
+ * memory: for hosts that keep every byte of device memory in their own pool
+ * and forbid a library from calling cudaMalloc (or cannot afford the
+ * device-wide synchronisation cudaMalloc/cudaFree may cause). Its two FP64
+ * vectors and reduction slots live in a static device array of the library
+ * (16 MiB + 512 bytes, held by every GPU that loads the library until exit),
+ * so n must be <= EXCENT_NOALLOC_MAX_N; larger graphs get EXCENT_ERR_ARG.
+ * The first call on a device looks the array's address up
+ * (cudaGetSymbolAddress) and should come before any stream capture. All
+ * calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller. No counterpart in the reference. */
+#define EXCENT_NOALLOC_MAX_N (1 << 20)
+int excent_params_fp64_noalloc(int device, int n, const unsigned long long* d_idx, const int32_t* d_adj,
+                               double katz_numerator, double* out, float* d_v1);
 /* FP64 reference solution on the device: kind 0 PageRank (x0 = 0.15,
  * x = 0.15 + 0.85 sum x_u / L(u)), 1 Katz (x = beta + alpha sum x_u),
  * 2 eigenvector (power iteration, unit L2 norm, sign fixed by the sum); Jacobi
