@@ -38,7 +38,9 @@ sys.path.insert(0, ROOT)
 CONFIGS = {
     # name: (scale, edge_factor, seed, measure)
     "cached-all": (24, 16, 2, "all"),
+    "pr24": (24, 16, 2, "pr"),
     "pr16": (16, 16, 1, "pr"),
+    "ppr256": (24, 16, 2, "ppr"),
 }
 
 
@@ -194,12 +196,7 @@ def run_ours(a, world, rank, local, dist):
     launches = eng.launches() - l0
     t = ev0.elapsed_time(ev1) / 1e3
     if dist:
-        tt = torch.tensor([t], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t = float(tt.item())
-        pp = torch.tensor([pushed], dtype=torch.float64, device="cuda")
-        dist.all_reduce(pp)
-        pushed_all = float(pp.item())
+        t, pushed_all = reduce_over_ranks(t, pushed, dist, "cuda")
     else:
         pushed_all = float(pushed)
     value = pushed_all / t / 1e9
@@ -227,12 +224,7 @@ def run_ours(a, world, rank, local, dist):
     te = ev0.elapsed_time(ev1) / 1e3
     te_wall = time.perf_counter() - w0
     if dist:
-        tt = torch.tensor([te], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        te = float(tt.item())
-        pp = torch.tensor([e_pushed], dtype=torch.float64, device="cuda")
-        dist.all_reduce(pp)
-        e_pushed = float(pp.item())
+        te, e_pushed = reduce_over_ranks(te, e_pushed, dist, "cuda")
 
     log(f"e2e: {a.steps} solves in {te:.3f}s")
     # roofline of the dominant kernel (push + its hub tail), per-kernel events on a profiled solve
@@ -285,6 +277,103 @@ def run_ours(a, world, rank, local, dist):
         result["cpu_baseline"] = cpu_baseline(n, idx_np, h_adj.numpy()[:m], meas, measure, lam)
     g.close()
     eng.close()
+    return result
+
+
+def ppr_queries(n, nq=256, seed=7, max_size=4096):
+    """Seed sets: sizes floor(exp(U[0, ln 4096])) clamped to [1, 4096], vertices uniform without replacement."""
+    rng = np.random.default_rng(seed)
+    sizes = np.clip(np.floor(np.exp(rng.uniform(0, np.log(max_size), nq))).astype(np.int64), 1, max_size)
+    return [np.sort(rng.choice(n, int(k), replace=False)).astype(np.int32) for k in sizes]
+
+
+def run_ppr(a, world, rank, local, dist):
+    """256 personalized PageRank queries: batched (autotuned width) against one-at-a-time seeded solves."""
+    import torch
+
+    import excent_b200 as X
+    torch.cuda.set_device(local)
+    scale, ef, seed, _ = CONFIGS[a.config]
+    scale = a.scale or scale
+    g = X.DeviceGraph(scale, ef, seed, device=local)
+    n, m = g.n, g.m
+    di, da, _ = g.device_ptrs()
+    d = 0.85
+    nq_all = 256
+    qs_all = ppr_queries(n, nq_all)
+    lo, hi = X.shard(nq_all, world, rank)  # queries shard by rank, no exchange
+    qs = qs_all[lo:hi]
+    vals = [(1 - d) / len(q) for q in qs]
+    eps = 1e-4 * (1 - d)
+    log(f"graph scale {scale}: n={n} m={m}; {len(qs)} queries on this rank")
+    best, table = X.autotune_batch(n, m, di, da, qs, vals, eps, "ppr", d, device=local)
+    log(f"autotune: per-query ms {table} -> B={best}")
+    b = X.Batch(n, m, di, da, best, "ppr", d, device=local)
+    st = torch.cuda.ExternalStream(b.stream())
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    b.seed(qs[:best], vals[:best], eps)   # warm-up (graph build)
+    b.solve()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0.record(st)
+    tot_e = 0
+    passes = []
+    for i in range(0, len(qs), best):
+        b.seed(qs[i:i + best], vals[i:i + best], eps)
+        s = b.solve()
+        tot_e += s["pushed_edges"]
+        passes.append(s["passes"])
+    ev1.record(st)
+    torch.cuda.synchronize()
+    t_batch = ev0.elapsed_time(ev1) / 1e3
+    xb = [b.read(j) for j in range(min(4, len(qs)))]
+    log(f"batched: {len(qs)} queries in {t_batch:.3f}s, passes {passes}")
+    # the same queries one at a time through the plain engine (seeded PageRank, full snapshot per pass)
+    meas = X.measures("pr", eps_pr=eps)
+    h_idx = torch.empty(n + 1, dtype=torch.int64, pin_memory=True)
+    g.download(h_idx, torch.empty(max(m, 1), dtype=torch.int32, pin_memory=True))
+    v0, e = X.plan_chunks(h_idx.numpy().view(np.uint64), X.chunk_cap(m))
+    eng = X.Engine(n, m, meas, v0, e, device=local)
+    eng.upload_device(di, da)
+    X.seed_engine(eng, qs[0], vals[0])
+    X.resume(eng)
+    se = torch.cuda.ExternalStream(eng.stream())
+    torch.cuda.synchronize()
+    ev0.record(se)
+    seq_e = 0
+    xs = []
+    for j, q in enumerate(qs):
+        X.seed_engine(eng, q, vals[j])
+        s = X.resume(eng)
+        seq_e += s.pushed
+        if j < 4:
+            xs.append(eng.read(0))
+    ev1.record(se)
+    torch.cuda.synchronize()
+    t_seq = ev0.elapsed_time(ev1) / 1e3
+    log(f"sequential: {len(qs)} queries in {t_seq:.3f}s")
+    diff = [float(np.abs(xb[j].astype(np.float64) - xs[j]).sum()) for j in range(len(xb))]
+    if dist:
+        tt = torch.tensor([t_batch, t_seq], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_batch, t_seq = float(tt[0]), float(tt[1])
+    result = {
+        "metric": "batched personalized PageRank solves/s (256 queries, eps 1e-4 x seed mass)",
+        "value": round(nq_all / t_batch, 3), "unit": "solves/s", "n_gpus": world, "steps": 1, "warmup": 1,
+        "ms_per_step": round(t_batch * 1e3, 3), "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded R-MAT, generated on the device; query seeds numpy seed 7)",
+        "config": {"workload": f"256-query PPR on R-MAT scale {scale} EF {ef} seed {seed}", "n": n, "m": m,
+                   "batch_width": best, "autotune_ms_per_query": table, "passes_per_batch": passes,
+                   "pushed_edges": int(tot_e), "queries_per_rank": len(qs)},
+        "sequential": {"solves_per_s": round(nq_all / t_seq, 3), "seconds": round(t_seq, 3),
+                       "pushed_edges": int(seq_e)},
+        "speedup_vs_sequential": round(t_seq / t_batch, 2),
+        "l1_batched_minus_sequential": diff,
+    }
+    b.close()
+    eng.close()
+    g.close()
     return result
 
 
@@ -356,12 +445,22 @@ def main():
         if res is not None:
             print(json.dumps(res))
         return
-    res = run_ours(a, world, rank, local, dist)
+    res = run_ppr(a, world, rank, local, dist) if CONFIGS[a.config][3] == "ppr" else run_ours(a, world, rank, local, dist)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(res))
+
+
+def reduce_over_ranks(t, units, dist, device):
+    """Job time = max over ranks; units = sum over ranks."""
+    import torch
+    tt = torch.tensor([float(t)], dtype=torch.float64, device=device)
+    uu = torch.tensor([float(units)], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    dist.all_reduce(uu)
+    return float(tt.item()), float(uu.item())
 
 
 if __name__ == "__main__":

@@ -355,3 +355,32 @@ def seed_engine(eng, vids, vals):
 def resume(eng, list_frac=0.5, max_passes=100000, use_graph=True):
     call("excent_engine_resume", eng.h, float(list_frac), int(max_passes), int(use_graph))
     return eng.stats()
+
+
+def _pack_queries(seeds, values, eps):
+    nq = len(seeds)
+    off = np.zeros(nq + 1, dtype=np.int32)
+    off[1:] = np.cumsum([len(s) for s in seeds])
+    vids = np.ascontiguousarray(np.concatenate(seeds), dtype=np.int32)
+    vals = np.ascontiguousarray(np.concatenate([np.broadcast_to(np.asarray(v, dtype=np.float32), (len(s),))
+                                                for s, v in zip(seeds, values)]), dtype=np.float32)
+    e = np.ascontiguousarray(np.broadcast_to(np.asarray(eps, dtype=np.float32), (nq,)))
+    return off, vids, vals, e
+
+
+def autotune_batch(n, m, d_idx, d_adj, seeds, values, eps, kind="ppr", d_or_alpha=0.85, device=0, max_passes=100000):
+    """Batch width with the lowest time per query on these queries (excent_batch_autotune)."""
+    off, vids, vals, e = _pack_queries(seeds, values, eps)
+    best = C.c_int()
+    ms = np.zeros(4, dtype=np.float64)
+    call("excent_batch_autotune", int(device), int(n), int(m), _ptr(d_idx), _ptr(d_adj), {"ppr": 0, "katz": 1}[kind],
+         float(d_or_alpha), len(seeds), _ptr(off), _ptr(vids), _ptr(vals), _ptr(e), int(max_passes), C.byref(best),
+         _tp(ms, _capi.f64p))
+    return best.value, dict(zip((32, 64, 128, 256), ms.tolist()))
+
+
+def shard(count, world, rank):
+    """Contiguous share [lo, hi) of `count` independent units (queries, replicas) for `rank` of `world`."""
+    lo = count * rank // world
+    hi = count * (rank + 1) // world
+    return lo, hi

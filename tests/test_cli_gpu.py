@@ -97,7 +97,8 @@ def test_cli_sample_matches_reference_binary(tmp_path):
         ours = run(CLI, args + ["--dump", str(tmp_path / "a")], tmp_path)
         ref = run(REF_CLI, args + ["--dump", str(tmp_path / "b")], tmp_path)
         # same line structure (first words of every line)
-        heads = lambda s: [re.sub(r"[-0-9.e+]+", "#", l)[:25] for l in s.splitlines() if not l.startswith("throughput")]  # noqa: E731
+        num = r"[-+]?\d+(?:\.\d+)?(?:e[-+]?\d+)?"
+        heads = lambda s: [re.sub(num, "#", l)[:25] for l in s.splitlines() if not l.startswith("throughput")]  # noqa: E731
         h1, h2 = heads(ours), heads(ref)
         assert h1[:4] == h2[:4]
         assert [l for l in h1 if l.startswith("passes")] and [l for l in h2 if l.startswith("passes")]
