@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--ev-project", default="on", choices=["on", "off"],
                     help="FP64 eigenvector normalisation step (remove the principal-eigenvector component of the "
                          "eigenvector residual each pass); the `all` run does not reach eps 1e-6 at scale 24 without it")
+    ap.add_argument("--pull-frac", type=float, default=0.3,
+                    help="gather passes when the pending demand >= this fraction of the edges (0: always scatter)")
     ap.add_argument("--ev-init", default="fp64", choices=["fp64", "reference"],
                     help="eigenvector initial residual from the FP64 lambda1 (default) or from lambda1 rounded to "
                          "float as the reference does")
@@ -171,6 +173,7 @@ def run_ours(a, world, rank, local, dist):
     eng.upload_device(d_idx, d_adj)
     if v1 is not None and a.ev_project == "on":
         eng.ev_project(v1)
+    eng.set_pull(a.pull_frac)
     use_graph = not a.no_graph
     for _ in range(a.warmup):
         s = eng.solve(use_graph=use_graph)
@@ -258,7 +261,8 @@ def run_ours(a, world, rank, local, dist):
                    "pushed_per_solve": int(pushed / a.steps), "time_to_eps_ms": round(t / a.steps * 1e3, 3),
                    "l2_note": "inputs larger than L2 (edge cache %.2f GB)" % (m * 4 / 1e9),
                    "cuda_graph": use_graph, "parallelism": f"{world} independent replicas",
-                   "ev_init": a.ev_init, "ev_project": a.ev_project if measure == "all" else None},
+                   "ev_init": a.ev_init, "ev_project": a.ev_project if measure == "all" else None,
+                   "pull_frac": a.pull_frac},
         "e2e": {"value": round(e_pushed / te / 1e9, 4), "unit": "GTEPS", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": round(te / a.steps * 1e3, 3),
                 "wall_ms_per_step": round(te_wall / a.steps * 1e3, 3)},

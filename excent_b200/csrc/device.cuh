@@ -53,6 +53,16 @@ template <typename T> __device__ __forceinline__ T warp_sum(T v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(FULL, v, o);
     return v;  // valid in lane 0
 }
+__device__ __forceinline__ float4 warp_sum(float4 v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_down_sync(FULL, v.x, o);
+        v.y += __shfl_down_sync(FULL, v.y, o);
+        v.z += __shfl_down_sync(FULL, v.z, o);
+        v.w += __shfl_down_sync(FULL, v.w, o);
+    }
+    return v;  // valid in lane 0
+}
 __device__ __forceinline__ unsigned warp_incl_scan(unsigned v, int lane) {
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {

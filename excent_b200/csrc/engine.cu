@@ -45,7 +45,7 @@ struct Ctrl {
     int pass;          // passes that pushed so far
     int done;          // 1 once a snapshot found nothing pending (or max passes)
     int err;           // nonzero: a device-side capacity check failed
-    int pad;
+    int pull;          // this pass gathers (pull) instead of scattering (push)
     double rsum[MAXM]; // FP64 sum |r| of the last snapshot
     unsigned hcount;   // hot pending list length
     unsigned pad2;
@@ -57,6 +57,7 @@ struct PassRec {
     ull pending, demand, hot_pending, pushed_before;
     double rsum[MAXM];
     int n_list, n_range;
+    int pull, pad;
 };
 
 struct SnapArgs {
@@ -280,7 +281,7 @@ __global__ void __launch_bounds__(BLOCK) k_snapshot(SnapArgs a) {
 // next snapshot accumulates into, and set the graph's loop condition.
 __global__ void k_plan(int nc, const int* cv0, int n, ull* cnt, const uint8_t* cmode, double list_frac, int max_passes,
                        uint8_t* wt_type, unsigned* wt_prefix, Ctrl* ctrl, ull* hub_cnt, PassRec* log, int log_cap,
-                       cudaGraphConditionalHandle cond, int use_cond) {
+                       cudaGraphConditionalHandle cond, int use_cond, double pull_edges) {
     __shared__ ull s_pend, s_dem;
     __shared__ unsigned s_carry;
     __shared__ int s_nl, s_nr;
@@ -296,12 +297,14 @@ __global__ void k_plan(int nc, const int* cv0, int n, ull* cnt, const uint8_t* c
     const ull pend = s_pend, dem = s_dem, hp = ctrl->hotpend;
     const int p = ctrl->pass;
     const bool stop = ctrl->done || p >= max_passes || (pend == 0 && hp == 0);
+    // dense pass: gather over every list instead of scattering the pending ones
+    const bool pull = !stop && pull_edges > 0 && (double)dem >= pull_edges;
     // work table, scanned in tiles of blockDim.x chunks
     for (int base = 0; base < nc; base += blockDim.x) {
         const int c = base + t;
         unsigned items = 0;
         uint8_t ty = WT_NONE;
-        if (!stop && c < nc && cmode[c] && cnt[2 * c] > 0) {
+        if (!stop && !pull && c < nc && cmode[c] && cnt[2 * c] > 0) {
             const int v0 = cv0[c], v1 = c + 1 < nc ? cv0[c + 1] : n;
             if ((double)cnt[2 * c] < list_frac * (v1 - v0)) { ty = WT_LIST; items = (unsigned)cnt[2 * c]; atomicAdd(&s_nl, 1); }
             else { ty = WT_RANGE; items = (unsigned)(v1 - v0); atomicAdd(&s_nr, 1); }
@@ -327,7 +330,9 @@ __global__ void k_plan(int nc, const int* cv0, int n, ull* cnt, const uint8_t* c
             R.pending = pend; R.demand = dem; R.hot_pending = hp; R.pushed_before = ctrl->pushed;
             for (int k = 0; k < MAXM; k++) R.rsum[k] = ctrl->rsum[k];
             R.n_list = s_nl; R.n_range = s_nr;
+            R.pull = pull;
         }
+        ctrl->pull = pull;
         ctrl->items = stop ? 0 : s_carry;
         if (stop) ctrl->done = 1; else ctrl->pass = p + 1;
         *hub_cnt = 0;
@@ -510,6 +515,192 @@ __global__ void __launch_bounds__(BLOCK) k_hub(void* rv, const HubSeg* q, const 
     }
 }
 
+// ---------------------------------------------------------------- pull pass
+// A dense pass (pending demand >= a set fraction of the edges) runs as a
+// gather on symmetric graphs: k_take takes every pending vertex's residual
+// (plain loads and stores: nothing else touches r during the take) and writes
+// its per-entry weight P[v] (zero when not pending), then k_pull adds to each
+// vertex the weights of its neighbours, r[v] += sum_{u in N(v)} P[u], which is
+// what the scatter of every pending vertex would add. Lists longer than
+// HUB_MIN are summed in HUB_SEG-entry segments by k_pullhub.
+template <int L>
+__global__ void __launch_bounds__(BLOCK) k_take(int n, void* xv, void* rv, void* Pv, const ull* idx, DevMeasures M,
+                                                Ctrl* ctrl) {
+    typedef typename Lane<L>::T T;
+    if (!ctrl->pull) return;
+    T* x = reinterpret_cast<T*>(xv);
+    T* r = reinterpret_cast<T*>(rv);
+    T* P = reinterpret_cast<T*>(Pv);
+    __shared__ ull s_pushed[BLOCK / 32];
+    ull pushed = 0;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
+        const ull deg = idx[v + 1] - idx[v];
+        T p;
+        if constexpr (L == 1) {
+            const float cur = r[v];
+            float d = 0.f;
+            if (fabsf(cur) > M.eps[0]) { d = cur; r[v] = 0.f; x[v] += d; }
+            p = deg ? weight(d, deg, M, 0) : 0.f;
+            if (d != 0.f && deg) pushed += deg;
+        } else {
+            float4 cur = r[v];
+            float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (fabsf(cur.x) > M.eps[0]) { d.x = cur.x; cur.x = 0.f; }
+            if (M.nm > 1 && fabsf(cur.y) > M.eps[1]) { d.y = cur.y; cur.y = 0.f; }
+            if (M.nm > 2 && fabsf(cur.z) > M.eps[2]) { d.z = cur.z; cur.z = 0.f; }
+            if (nonzero(d)) {
+                r[v] = cur;
+                float4 xv4 = x[v];
+                xv4.x += d.x; xv4.y += d.y; xv4.z += d.z;
+                x[v] = xv4;
+                if (deg) pushed += deg;
+            }
+            p = deg ? make_float4(weight(d.x, deg, M, 0), weight(d.y, deg, M, 1), weight(d.z, deg, M, 2), 0.f)
+                    : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        P[v] = p;
+    }
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    pushed = warp_sum(pushed);
+    if (lane == 0) s_pushed[wib] = pushed;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ull t = 0;
+        for (int i = 0; i < BLOCK / 32; i++) t += s_pushed[i];
+        if (t) atomicAdd(&ctrl->pushed, t);
+    }
+}
+
+__device__ __forceinline__ float shfl_up(float v, int d) { return __shfl_up_sync(FULL, v, d); }
+__device__ __forceinline__ float4 shfl_up(float4 v, int d) {
+    return make_float4(__shfl_up_sync(FULL, v.x, d), __shfl_up_sync(FULL, v.y, d), __shfl_up_sync(FULL, v.z, d),
+                       __shfl_up_sync(FULL, v.w, d));
+}
+__device__ __forceinline__ void acc_add(float& a, float b) { a += b; }
+__device__ __forceinline__ void acc_add(float4& a, float4 b) { a.x += b.x; a.y += b.y; a.z += b.z; a.w += b.w; }
+template <typename T> __device__ __forceinline__ T zero_of();
+template <> __device__ __forceinline__ float zero_of<float>() { return 0.f; }
+template <> __device__ __forceinline__ float4 zero_of<float4>() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+
+template <int L>
+__global__ void __launch_bounds__(BLOCK) k_pull(int n, void* rv, const void* Pv, const ull* idx, const int* cache,
+                                                HubSeg* hubq, ull* hub_cnt, ull hub_cap, Ctrl* ctrl) {
+    typedef typename Lane<L>::T T;
+    if (!ctrl->pull) return;
+    T* r = reinterpret_cast<T*>(rv);
+    const T* P = reinterpret_cast<const T*>(Pv);
+    __shared__ const int* s_nb[BLOCK / 32][32];
+    __shared__ unsigned s_ex[BLOCK / 32][32];
+    __shared__ T s_acc[BLOCK / 32][32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long tile = gw; tile * 32 < n; tile += nwarps) {
+        const long long v = tile * 32 + lane;
+        ull b = 0, deg = 0;
+        if (v < n) { b = idx[v]; deg = idx[v + 1] - b; }
+        const int* nb = cache + b;
+        const bool large = deg > HUB_MIN;
+        if (large) {
+            const unsigned nseg = (unsigned)((deg + HUB_SEG - 1) / HUB_SEG);
+            const ull base = atomicAdd(hub_cnt, (ull)nseg);
+            if (base + nseg <= hub_cap) {
+                for (unsigned s = 0; s < nseg; s++) {
+                    HubSeg h;
+                    h.nb = nb + (ull)s * HUB_SEG;
+                    h.len = (unsigned)min((ull)HUB_SEG, deg - (ull)s * HUB_SEG);
+                    h.pad = (unsigned)v;
+                    h.p = make_float4(0.f, 0.f, 0.f, 0.f);
+                    hubq[base + s] = h;
+                }
+            } else {
+                atomicExch(&ctrl->err, 1);
+            }
+        }
+        const unsigned ds = large ? 0u : (unsigned)deg;
+        const unsigned incl = warp_incl_scan(ds, lane);
+        const unsigned tot = __shfl_sync(FULL, incl, 31);
+        if (!tot) continue;
+        s_nb[wib][lane] = nb;
+        s_ex[wib][lane] = incl - ds;
+        s_acc[wib][lane] = zero_of<T>();
+        __syncwarp();
+        for (unsigned j0 = 0; j0 < tot; j0 += 32 * UNROLL) {
+            T val[UNROLL];
+            int own[UNROLL];
+#pragma unroll
+            for (int k = 0; k < UNROLL; k++) {
+                const unsigned j = j0 + 32 * k + lane;
+                int lo = 0;
+#pragma unroll
+                for (int step = 16; step > 0; step >>= 1) {
+                    const unsigned vl = __shfl_sync(FULL, incl, lo + step - 1);
+                    if (vl <= j) lo += step;
+                }
+                own[k] = j < tot ? lo : -1;
+                val[k] = zero_of<T>();
+                if (j < tot) val[k] = P[ld_edge(s_nb[wib][lo] + (j - s_ex[wib][lo]))];
+            }
+#pragma unroll
+            for (int k = 0; k < UNROLL; k++) {
+                // segmented inclusive sum over lanes with the same owner (owners ascend with the lane)
+                T sv = val[k];
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const T t = shfl_up(sv, d);
+                    const int od = __shfl_up_sync(FULL, own[k], d);
+                    if (lane >= d && od == own[k]) acc_add(sv, t);
+                }
+                const int nxt = __shfl_down_sync(FULL, own[k], 1);
+                if (own[k] >= 0 && (lane == 31 || nxt != own[k])) acc_add(s_acc[wib][own[k]], sv);
+                __syncwarp();
+            }
+        }
+        if (ds) {
+            const T add = s_acc[wib][lane];
+            if (nonzero(add)) {
+                T cur = r[v];
+                acc_add(cur, add);
+                r[v] = cur;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+template <int L>
+__global__ void __launch_bounds__(BLOCK) k_pullhub(void* rv, const void* Pv, const HubSeg* q, const ull* hub_cnt,
+                                                   ull cap, const Ctrl* ctrl) {
+    typedef typename Lane<L>::T T;
+    if (!ctrl->pull) return;
+    T* r = reinterpret_cast<T*>(rv);
+    const T* P = reinterpret_cast<const T*>(Pv);
+    const int lane = threadIdx.x & 31;
+    const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    ull cnt = *hub_cnt;
+    if (cnt > cap) cnt = cap;
+    for (long long s = gw; s < (long long)cnt; s += nwarps) {
+        const HubSeg h = q[s];
+        T acc = zero_of<T>();
+        const unsigned mis = (unsigned)(((uintptr_t)h.nb >> 2) & 3u);
+        unsigned head = (4u - mis) & 3u;
+        if (head > h.len) head = h.len;
+        if (lane < (int)head) acc_add(acc, P[ld_edge(h.nb + lane)]);
+        const int4* body = reinterpret_cast<const int4*>(h.nb + head);
+        const unsigned nbody = (h.len - head) >> 2;
+        for (unsigned i = lane; i < nbody; i += 32) {
+            const int4 e = ld_edge4(body + i);
+            const T a0 = P[e.x], a1 = P[e.y], a2 = P[e.z], a3 = P[e.w];
+            acc_add(acc, a0); acc_add(acc, a1); acc_add(acc, a2); acc_add(acc, a3);
+        }
+        const unsigned tail = (h.len - head) & 3u;
+        if (lane < (int)tail) acc_add(acc, P[ld_edge(h.nb + head + nbody * 4 + lane)]);
+        acc = warp_sum(acc);
+        if (lane == 0 && nonzero(acc)) red_add(r, (int)h.pad, acc);
+    }
+}
+
 // Pending hot vertices among hot ids [lo, hi) at launch time, appended with
 // one global atomic per block (src/excent.cu:178-182).
 template <int L>
@@ -610,6 +801,8 @@ struct excent_engine {
     bool trace_on = false;
     float* d_tmp = nullptr;  // n floats for readback of the float4 layout
     float* d_v1 = nullptr;   // unit principal eigenvector for the EV normalisation step
+    void* d_P = nullptr;     // per-vertex push weights of a pull pass
+    double pull_frac = 0;    // pull when the pending demand >= pull_frac * m (0: never)
     bool ev_proj = false;
     int ev_index = -1;
     int* d_cache = nullptr;
@@ -658,7 +851,7 @@ static int free_engine(excent_engine* e) {
     cudaDeviceSynchronize();
     if (e->gexec) cudaGraphExecDestroy(e->gexec);
     if (e->graph) cudaGraphDestroy(e->graph);
-    void* dptrs[] = {e->d_v1, e->d_idx, e->d_x, e->d_r, e->d_bitmap, e->d_cnt, e->d_cv0, e->d_list, e->d_ctrl, e->d_cmode,
+    void* dptrs[] = {e->d_P, e->d_v1, e->d_idx, e->d_x, e->d_r, e->d_bitmap, e->d_cnt, e->d_cv0, e->d_list, e->d_ctrl, e->d_cmode,
                      e->d_wt_type, e->d_wt_prefix, e->d_hubq[0], e->d_hubq[1], e->d_hubq[2], e->d_hubcnt, e->d_log, e->d_trace, e->d_tmp, e->d_cache,
                      e->d_hids, e->d_hoff, e->d_hedges, e->d_hot, e->d_hlist};
     for (void* p : dptrs) if (p) cudaFree(p);
@@ -1217,22 +1410,39 @@ static void enqueue_pass(excent_engine* e, double list_frac, int max_passes, cud
     if (ev) cudaEventRecord(ev[0], st);
     launch_snapshot(e, false, st);
     if (ev) cudaEventRecord(ev[1], st);
+    const double pull_edges = e->pull_frac > 0 && e->d_P ? e->pull_frac * (double)e->m : 0.0;
     k_plan<<<1, 1024, 0, st>>>(e->nc, e->d_cv0, e->n, e->d_cnt, e->d_cmode, list_frac, max_passes, e->d_wt_type,
-                               e->d_wt_prefix, e->d_ctrl, e->d_hubcnt, e->d_log, e->log_cap, cond, use_cond);
+                               e->d_wt_prefix, e->d_ctrl, e->d_hubcnt, e->d_log, e->log_cap, cond, use_cond,
+                               pull_edges);
     e->launches++;
     if (ev) cudaEventRecord(ev[2], st);
     PushArgs a = push_args(e, 0);
-    if (!ev) {
-        launch_push<SRC_TABLE>(e, a, e->grid_push, st);
-        return;
-    }
+    const int gt = e->sms * 8;
     if (e->L == 1) k_push<1, SRC_TABLE><<<e->grid_push, BLOCK, 0, st>>>(a);
     else k_push<4, SRC_TABLE><<<e->grid_push, BLOCK, 0, st>>>(a);
-    cudaEventRecord(ev[3], st);
+    e->launches++;
+    if (pull_edges > 0) {   // each of these returns at once unless k_plan chose a pull pass
+        if (e->L == 1) {
+            k_take<1><<<gt, BLOCK, 0, st>>>(e->n, e->d_x, e->d_r, e->d_P, e->d_idx, e->M, e->d_ctrl);
+            k_pull<1><<<e->grid_push, BLOCK, 0, st>>>(e->n, e->d_r, e->d_P, e->d_idx, e->d_cache, a.hubq, a.hub_cnt,
+                                                       a.hub_cap, e->d_ctrl);
+        } else {
+            k_take<4><<<gt, BLOCK, 0, st>>>(e->n, e->d_x, e->d_r, e->d_P, e->d_idx, e->M, e->d_ctrl);
+            k_pull<4><<<e->grid_push, BLOCK, 0, st>>>(e->n, e->d_r, e->d_P, e->d_idx, e->d_cache, a.hubq, a.hub_cnt,
+                                                       a.hub_cap, e->d_ctrl);
+        }
+        e->launches += 2;
+    }
+    if (ev) cudaEventRecord(ev[3], st);
     if (e->L == 1) k_hub<1><<<e->grid_push, BLOCK, 0, st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap);
     else k_hub<4><<<e->grid_push, BLOCK, 0, st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap);
-    cudaEventRecord(ev[4], st);
-    e->launches += 2;
+    e->launches++;
+    if (pull_edges > 0) {
+        if (e->L == 1) k_pullhub<1><<<e->grid_push, BLOCK, 0, st>>>(e->d_r, e->d_P, a.hubq, a.hub_cnt, a.hub_cap, e->d_ctrl);
+        else k_pullhub<4><<<e->grid_push, BLOCK, 0, st>>>(e->d_r, e->d_P, a.hubq, a.hub_cnt, a.hub_cap, e->d_ctrl);
+        e->launches++;
+    }
+    if (ev) cudaEventRecord(ev[4], st);
 }
 
 static int build_graph(excent_engine* e, double list_frac, int max_passes) {
@@ -1319,7 +1529,7 @@ static int solve_impl(excent_engine* e, double list_frac, int max_passes, int us
         EX_CUDA(cudaGraphLaunch(e->gexec, e->s_main));
         EX_CUDA(cudaStreamSynchronize(e->s_main));
         EX_CUDA(cudaMemcpy(e->h_ctrl, e->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
-        e->launches += 4ull * (e->h_ctrl->pass + 1);
+        e->launches += (e->pull_frac > 0 && e->d_P ? 7ull : 4ull) * (e->h_ctrl->pass + 1);
     } else {
         for (int p = 0; p <= max_passes; p++) {
             enqueue_pass(e, list_frac, max_passes, 0, 0, e->s_main, e->prof ? e->ev : nullptr);
@@ -1368,6 +1578,7 @@ extern "C" int excent_engine_stats(excent_engine* e, excent_stats* st, excent_pa
             L.pushed = (p + 1 < np ? recs[p + 1].pushed_before : c.pushed) - recs[p].pushed_before;
             for (int k = 0; k < MAXM; k++) L.rsum[k] = recs[p].rsum[k];
             L.n_list = recs[p].n_list; L.n_range = recs[p].n_range;
+            L.pull = recs[p].pull;
         }
     }
     return EXCENT_OK;
@@ -1422,6 +1633,15 @@ extern "C" int excent_device_info(int device, excent_device_info_t* out) {
     EX_CUDA(cudaDeviceGetAttribute(&out->sms, cudaDevAttrMultiProcessorCount, device));
     EX_CUDA(cudaDeviceGetAttribute(&out->cc_major, cudaDevAttrComputeCapabilityMajor, device));
     EX_CUDA(cudaDeviceGetAttribute(&out->cc_minor, cudaDevAttrComputeCapabilityMinor, device));
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_set_pull(excent_engine* e, double pull_frac) {
+    EX_CHECK_ARG(e && pull_frac >= 0, "bad argument");
+    EX_CUDA(cudaSetDevice(e->dev));
+    invalidate_graph(e);
+    if (pull_frac > 0 && !e->d_P) EX_ALLOC(e->d_P, (size_t)e->n * (e->L == 1 ? sizeof(float) : sizeof(float4)));
+    e->pull_frac = pull_frac;
     return EXCENT_OK;
 }
 

@@ -188,6 +188,7 @@ typedef struct excent_pass_log {
     unsigned long long pushed;    /* adjacency entries pushed in the pass */
     double rsum[3];               /* FP64 sum of |r| per measure at the snapshot */
     int n_list, n_range;          /* chunks pushed as lists / whole ranges */
+    int pull;                     /* 1: the pass ran as a gather (excent_engine_set_pull) */
 } excent_pass_log;
 
 typedef struct excent_stats {
@@ -212,6 +213,15 @@ int excent_engine_write(excent_engine* e, int i, const float* x, const float* r)
  * pending (src/excent.cu:76, 606-607, 779-789). enable before init. */
 int excent_engine_trace(excent_engine* e, int enable);
 int excent_engine_read_trace(excent_engine* e, uint16_t* out);
+
+/* Direction-optimised passes for the device solve on a SYMMETRIC graph (every
+ * edge stored in both directions): a pass whose pending demand (sum of
+ * pending degrees) is at least pull_frac * m runs as a gather. It takes every
+ * pending vertex (no concurrent updates in that pass), writes its per-entry
+ * weight, then adds to each vertex the weights of its neighbours: the sum the
+ * scatter would have added, without atomics. 0 turns it off (the default).
+ * No reference counterpart: the reference always scatters. */
+int excent_engine_set_pull(excent_engine* e, double pull_frac);
 
 /* FP64 eigenvector normalisation step: with the unit principal eigenvector
  * v1 (n floats, host or device pointer; NULL turns it off), every snapshot

@@ -244,8 +244,9 @@ def test_rmat_generator_bitexact_vs_oracle():
         g.close()
 
 
+@pytest.mark.parametrize("pull", [0.0, 0.3])
 @pytest.mark.parametrize("measure", ["pr", "katz", "ev", "all"])
-def test_error_no_looser_than_reference_engine(sample, measure):
+def test_error_no_looser_than_reference_engine(sample, measure, pull):
     """The reference engine's own result dumps on the sample (built from its
     source and run on a B200, committed under tests/golden/) against the
     reference's FP64 oracle vectors: our L1 and max errors must not be looser."""
@@ -254,7 +255,11 @@ def test_error_no_looser_than_reference_engine(sample, measure):
     names = ["pr", "katz", "ev"] if measure == "all" else [measure]
     meas = meas_for(measure, env)
     eng = make_engine(n, idx, adj, meas)
-    eng.solve()
+    eng.set_pull(pull)
+    st, log = eng.solve(), None
+    st, log = eng.stats(with_log=True)
+    if pull:
+        assert any(l.pull for l in log)
     for i, k in enumerate(names):
         p = os.path.join(GOLDEN, f"sample_excent_{measure}_{k}.f32")
         ref = np.fromfile(os.path.join(GOLDEN, f"sample_ref_{k}.f64"))
@@ -289,3 +294,32 @@ def test_ev_normalisation_step_keeps_the_unit_eigenvector(rmat16):
         assert st.passes < 5000
         assert c["l1_rel"] < 2e-3 and c["top1000"] >= 990
         eng.close()
+
+
+@pytest.mark.parametrize("measure", ["pr", "all"])
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_pull_passes_match_push(rmat16, measure, use_graph):
+    """Dense passes as gathers (symmetric graph) reach the same fixed point."""
+    n, idx, adj = rmat16
+    par = O.params(n, idx, adj)
+    kw = dict(alpha=0.9 / par["_lambda"], lam=par["_lambda"], eps_katz=1e-5, eps_ev=1e-5) if measure == "all" else {}
+    names = ["pr", "katz", "ev"] if measure == "all" else ["pr"]
+    res = {}
+    for pull in (0.0, 0.3):
+        meas = X.measures(measure, **kw)
+        eng = make_engine(n, idx, adj, meas)
+        eng.set_pull(pull)
+        st = eng.solve(use_graph=use_graph)
+        st, log = eng.stats(with_log=True)
+        assert sum(l.pull for l in log) > (0 if pull else -1)
+        if not pull:
+            assert not any(l.pull for l in log)
+        for i, k in enumerate(names):
+            r = eng.read(i, residual=True)
+            assert np.all(np.abs(r) <= np.float32(meas.eps[i]))
+            ref = O.reference_solution(n, idx, adj, k, alpha=kw.get("alpha"))
+            res[(pull, k)] = O.compare(k, ref, eng.read(i))
+        eng.close()
+    for k in names:
+        print(k, "push", res[(0.0, k)], "pull", res[(0.3, k)])
+        assert res[(0.3, k)]["l1_rel"] <= 1.1 * res[(0.0, k)]["l1_rel"] + 1e-7
