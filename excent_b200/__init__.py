@@ -311,6 +311,9 @@ class Batch:
         call("excent_batch_seed", self.h, nq, _ptr(off), _ptr(vids) if len(vids) else None,
              _ptr(vals) if len(vals) else None, _ptr(e))
 
+    def set_greedy(self, greedy=True):
+        call("excent_batch_set_greedy", self.h, int(greedy))
+
     def solve(self, max_passes=100000, use_graph=True):
         call("excent_batch_solve", self.h, int(max_passes), int(use_graph))
         return self.stats()

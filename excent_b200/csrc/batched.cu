@@ -66,6 +66,7 @@ struct BArgs {
     BSeg* seg;
     ull seg_cap;
     BCtrl* ctrl;
+    int greedy;               // take every nonzero lane of a pushed row, not only the pending ones
 };
 
 __device__ __forceinline__ void mark(uint32_t* t, int u) {
@@ -128,16 +129,28 @@ __global__ void __launch_bounds__(BB) k_bpass(BArgs a) {
             float4* rrow = a.R + (size_t)v * a.V;
             float4 d[NV];
             bool any = false;
+            // a row with any pending lane is pushed whole (greedy): every lane with a nonzero
+            // residual is taken, since the one read of the list serves them all
+            float4 rv[NV];
+            bool pend = false;
+#pragma unroll
+            for (int k = 0; k < NV; k++) {
+                rv[k] = lane < LPR ? rrow[j0 + LPR * k] : make_float4(0.f, 0.f, 0.f, 0.f);
+                pend |= fabsf(rv[k].x) > eps[k].x || fabsf(rv[k].y) > eps[k].y || fabsf(rv[k].z) > eps[k].z ||
+                        fabsf(rv[k].w) > eps[k].w;
+            }
+            const bool row_pend = __any_sync(FULL, pend);
+            const float4 floor0 = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
             for (int k = 0; k < NV; k++) {
                 d[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (lane < LPR) {
-                    const float4 rv = rrow[j0 + LPR * k];
+                if (lane < LPR && row_pend) {
+                    const float4 th = a.greedy ? floor0 : eps[k];
                     float* rp = reinterpret_cast<float*>(rrow + j0 + LPR * k);
-                    d[k].x = take_lane(rp, rv.x, eps[k].x);
-                    d[k].y = take_lane(rp + 1, rv.y, eps[k].y);
-                    d[k].z = take_lane(rp + 2, rv.z, eps[k].z);
-                    d[k].w = take_lane(rp + 3, rv.w, eps[k].w);
+                    d[k].x = take_lane(rp, rv[k].x, th.x);
+                    d[k].y = take_lane(rp + 1, rv[k].y, th.y);
+                    d[k].z = take_lane(rp + 2, rv[k].z, th.z);
+                    d[k].w = take_lane(rp + 3, rv[k].w, th.w);
                     if (nonzero(d[k])) {
                         float4* xp = a.X + (size_t)v * a.V + j0 + LPR * k;
                         float4 xv = *xp;
@@ -305,6 +318,7 @@ struct excent_batch {
     int graph_max = -1;
     int grid = 0;
     ull launches = 0;
+    int greedy = 1;
 };
 
 static void batch_free(excent_batch* b) {
@@ -332,6 +346,7 @@ static BArgs bargs(excent_batch* b) {
     a.words = (int)(((size_t)b->n + 31) / 32);
     a.P = b->d_P; a.prow_cap = b->prow_cap; a.seg = b->d_seg; a.seg_cap = b->seg_cap;
     a.ctrl = b->d_ctrl;
+    a.greedy = b->greedy;
     return a;
 }
 
@@ -529,6 +544,15 @@ extern "C" int excent_batch_read(excent_batch* b, int lane, int residual, float*
     EX_CUDA(cudaGetLastError());
     EX_CUDA(cudaMemcpyAsync(out, b->d_col, (size_t)b->n * sizeof(float), cudaMemcpyDeviceToHost, b->st));
     EX_CUDA(cudaStreamSynchronize(b->st));
+    return EXCENT_OK;
+}
+
+extern "C" int excent_batch_set_greedy(excent_batch* b, int greedy) {
+    EX_CHECK_ARG(b, "null batch");
+    b->greedy = greedy != 0;
+    if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
+    if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+    b->graph_max = -1;
     return EXCENT_OK;
 }
 

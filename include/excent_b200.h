@@ -346,6 +346,11 @@ int excent_batch_stats(excent_batch* b, int* passes, unsigned long long* pushed_
 /* Values (or residuals) of lane q for all n vertices, to host float32. */
 int excent_batch_read(excent_batch* b, int lane, int residual, float* out);
 int excent_batch_stream(excent_batch* b, void** stream);
+/* greedy (default 1): when a vertex has any pending lane, push every lane of
+ * its row whose residual is nonzero, since the one read of its list serves
+ * them all; 0: push only the pending lanes. Either way every lane ends with
+ * |r| <= eps. */
+int excent_batch_set_greedy(excent_batch* b, int greedy);
 /* Autotuner: time one batch of min(B, nq) of the given queries (seeded as
  * in excent_batch_seed) at each width B in {32, 64, 128, 256} and return the
  * width with the lowest time per query; per_query_ms[4] gets the times. */
