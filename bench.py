@@ -69,6 +69,11 @@ def parse():
                          "eigenvector residual each pass); the `all` run does not reach eps 1e-6 at scale 24 without it")
     ap.add_argument("--pull-frac", type=float, default=0.0,
                     help="gather passes when the pending demand >= this fraction of the edges (0: always scatter)")
+    ap.add_argument("--ref-gpu", action="store_true",
+                    help="also run this repo's CLI and the reference CLI (built from source) on the same EGR file")
+    ap.add_argument("--ref-passes", type=int, default=200, help="pass cap of the CLI runs for 'all'")
+    ap.add_argument("--hub-targets", type=int, default=0,
+                    help="shared-memory aggregation of the k highest-degree targets (0: off)")
     ap.add_argument("--ev-init", default="fp64", choices=["fp64", "reference"],
                     help="eigenvector initial residual from the FP64 lambda1 (default) or from lambda1 rounded to "
                          "float as the reference does")
@@ -175,6 +180,7 @@ def run_ours(a, world, rank, local, dist):
     if v1 is not None and a.ev_project == "on":
         eng.ev_project(v1)
     eng.set_pull(a.pull_frac)
+    eng.set_hub_targets(a.hub_targets)
     use_graph = not a.no_graph
     for _ in range(a.warmup):
         s = eng.solve(use_graph=use_graph)
@@ -263,7 +269,7 @@ def run_ours(a, world, rank, local, dist):
                    "l2_note": "inputs larger than L2 (edge cache %.2f GB)" % (m * 4 / 1e9),
                    "cuda_graph": use_graph, "parallelism": f"{world} independent replicas",
                    "ev_init": a.ev_init, "ev_project": a.ev_project if measure == "all" else None,
-                   "pull_frac": a.pull_frac},
+                   "pull_frac": a.pull_frac, "hub_targets": a.hub_targets},
         "e2e": {"value": round(e_pushed / te / 1e9, 4), "unit": "GTEPS", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": round(te / a.steps * 1e3, 3),
                 "wall_ms_per_step": round(te_wall / a.steps * 1e3, 3)},
@@ -280,6 +286,8 @@ def run_ours(a, world, rank, local, dist):
     log(f"profiled solve: {prof}")
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(n, idx_np, h_adj.numpy()[:m], meas, measure, lam)
+    if rank == 0 and world == 1 and a.ref_gpu:
+        result["cli_vs_reference_gpu"] = cli_compare(a, idx_np, h_adj.numpy()[:m], measure, meas, lam, local)
     g.close()
     eng.close()
     return result
@@ -473,6 +481,62 @@ def cpu_sample(n, idx, adj, meas, measure, lam, max_edges):
     _, _, passes, pushed = O.delta_push(n, idx, np.ascontiguousarray(adj), kinds, cv0=cv0, eps_pr=float(meas.eps[0]),
                                         max_edges=max_edges, threads=os.cpu_count(), **kw)
     return pushed, passes, time.perf_counter() - t0
+
+
+def cli_runs(binary, args, reps=2):
+    """Run a CLI `reps` times; keep the run with the shortest pass time."""
+    import re
+    import subprocess
+    best = None
+    for _ in range(reps):
+        r = subprocess.run([binary, *args], capture_output=True, text=True, timeout=1800)
+        if r.returncode != 0:
+            return {"error": (r.stderr or r.stdout)[-300:]}
+        out = r.stdout
+        passes = int(re.search(r"^passes (\d+)", out, re.M).group(1))
+        xe = float(re.search(r"edges pushed: ([0-9.]+) x", out).group(1))
+        tp = float(re.search(r"time: .* passes ([0-9.]+)s", out).group(1))
+        if best is None or tp < best["passes_s"]:
+            best = {"passes": passes, "pushed_x_m": xe, "passes_s": tp}
+    return best
+
+
+def cli_compare(a, idx, adj, measure, meas, lam, device):
+    """The same EGR file and flags through this repo's CLI and through the reference CLI
+    (src/excent.cu built from source by oracle/Makefile), both on this GPU. GTEPS =
+    edges pushed / pass-loop time as each CLI prints them."""
+    import shutil
+    import tempfile
+
+    import excent_b200 as X
+    import excent_b200._capi as K
+    ref_bin = os.path.join(ROOT, "oracle", "_ref", "excent")
+    if not os.path.exists(ref_bin):
+        return {"unavailable": "reference CLI not built (oracle/Makefile)"}
+    d = tempfile.mkdtemp(prefix="excent_bench_")
+    try:
+        path = os.path.join(d, "g.egr")
+        X.write_egr(path, idx, adj)
+        m = len(adj)
+        args = [path, "--measure", measure, "--stream-ratio", "2", "--cache", "chunks", "--count-pushes"]
+        if measure == "all":
+            args += ["--alpha", "%.9g" % (0.9 / lam), "--beta", "1", "--lambda", "%.17g" % lam,
+                     "--eps-katz", "1e-6", "--eps-ev", "1e-6", "--max-passes", str(a.ref_passes)]
+        env_dev = {"CUDA_VISIBLE_DEVICES": os.environ.get("CUDA_VISIBLE_DEVICES", str(device))}
+        os.environ.update(env_dev)
+        res = {"args": " ".join(args[1:]), "file_gb": round(os.path.getsize(path) / 1e9, 3)}
+        for name, binary, extra in (("reference", ref_bin, []), ("ours", K.CLI_PATH, []),
+                                    ("ours_device_loop", K.CLI_PATH, ["--device-loop"])):
+            r = cli_runs(binary, args + extra)
+            if "passes_s" in r:
+                r["gteps"] = round(r["pushed_x_m"] * m / r["passes_s"] / 1e9, 3)
+            res[name] = r
+            log(f"CLI {name}: {r}")
+        if "gteps" in res["reference"] and "gteps" in res["ours"]:
+            res["speedup_passes_time"] = round(res["reference"]["passes_s"] / res["ours"]["passes_s"], 3)
+        return res
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
 
 
 def cpu_baseline(n, idx, adj, meas, measure, lam):

@@ -201,6 +201,10 @@ class Engine:
     def results(self):
         return [self.read(i) for i in range(self.meas.nm)]
 
+    def set_hub_targets(self, k):
+        """Shared-memory aggregation of the contributions to the k highest-degree targets (0: off)."""
+        call("excent_engine_set_hub_targets", self.h, int(k))
+
     def set_pull(self, frac):
         """Gather passes when the pending demand >= frac * m (symmetric graphs only; 0 = never)."""
         call("excent_engine_set_pull", self.h, float(frac))
@@ -224,6 +228,25 @@ class Engine:
         p = C.c_uint64()
         call("excent_engine_profile_read", self.h, _tp(ms, _capi.f64p), C.byref(p))
         return dict(zip(("snapshot", "plan", "push", "hub"), ms.tolist())), p.value
+
+
+def write_egr(path, idx, adj, wide=True):
+    """Write a CSR graph as an EGR file (README.md:136-146): int32 n, then int32 -1 and int64 m
+    with uint64 offsets (wide), or int32 m with uint32 offsets (narrow); then int32 lists."""
+    idx = np.asarray(idx)
+    adj = np.asarray(adj)
+    n = len(idx) - 1
+    with open(path, "wb") as f:
+        if wide:
+            f.write(np.array([n, -1], dtype="<i4").tobytes())
+            f.write(np.array([len(adj)], dtype="<i8").tobytes())
+            f.write(np.ascontiguousarray(idx, dtype="<u8").tobytes())
+        else:
+            if len(adj) >= 2 ** 31:
+                raise ValueError("narrow EGR holds fewer than 2^31 entries")
+            f.write(np.array([n, len(adj)], dtype="<i4").tobytes())
+            f.write(np.ascontiguousarray(idx, dtype="<u4").tobytes())
+        f.write(np.ascontiguousarray(adj, dtype="<i4").tobytes())
 
 
 def params_fp64(n, d_idx, d_adj, katz_numerator=0.85, device=0, v1_out=None):

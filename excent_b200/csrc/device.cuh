@@ -119,33 +119,50 @@ __device__ __forceinline__ float4 take(float4* x, float4* r, int v, ull deg, con
 }
 
 __device__ __forceinline__ int ld_edge(const int* p) { return __ldcs(p); }
+
+// Hub-target aggregation: in an encoded edge cache an entry < 0 names slot
+// (entry & HUB_MASK) of a high-degree target; its contributions are summed in
+// the CTA's shared accumulators (hacc) and flushed once per CTA.
+static constexpr int HUB_MASK = 0x7fffffff;
+__device__ __forceinline__ void hacc_add(float* hacc, int slot, float p) { atomicAdd(hacc + slot, p); }
+__device__ __forceinline__ void hacc_add(float4* hacc, int slot, float4 p) {
+    float* h = reinterpret_cast<float*>(hacc + slot);
+    if (p.x != 0.f) atomicAdd(h, p.x);
+    if (p.y != 0.f) atomicAdd(h + 1, p.y);
+    if (p.z != 0.f) atomicAdd(h + 2, p.z);
+}
+template <typename P>
+__device__ __forceinline__ void scatter_one(P* r, int u, P p, P* hacc) {
+    if (u < 0) hacc_add(hacc, u & HUB_MASK, p);
+    else red_add(r, u, p);
+}
 __device__ __forceinline__ int4 ld_edge4(const int4* p) { return __ldcs(p); }
 
 // All 32 lanes scatter one adjacency list nb[0..deg): peel to a 16-byte
 // boundary, then 128-bit loads, then the tail.
 template <typename P>
-__device__ __forceinline__ void warp_scatter(P* r, const int* nb, unsigned deg, P p, int lane) {
+__device__ __forceinline__ void warp_scatter(P* r, const int* nb, unsigned deg, P p, int lane, P* hacc) {
     const unsigned mis = (unsigned)(((uintptr_t)nb >> 2) & 3u);
     unsigned head = (4u - mis) & 3u;
     if (head > deg) head = deg;
-    if (lane < (int)head) red_add(r, ld_edge(nb + lane), p);
+    if (lane < (int)head) scatter_one(r, ld_edge(nb + lane), p, hacc);
     const int4* body = reinterpret_cast<const int4*>(nb + head);
     const unsigned nbody = (deg - head) >> 2;
     unsigned i = lane;
     for (; i + 96 < nbody; i += 128) {  // four 128-bit loads in flight per lane
         const int4 q0 = ld_edge4(body + i), q1 = ld_edge4(body + i + 32);
         const int4 q2 = ld_edge4(body + i + 64), q3 = ld_edge4(body + i + 96);
-        red_add(r, q0.x, p); red_add(r, q0.y, p); red_add(r, q0.z, p); red_add(r, q0.w, p);
-        red_add(r, q1.x, p); red_add(r, q1.y, p); red_add(r, q1.z, p); red_add(r, q1.w, p);
-        red_add(r, q2.x, p); red_add(r, q2.y, p); red_add(r, q2.z, p); red_add(r, q2.w, p);
-        red_add(r, q3.x, p); red_add(r, q3.y, p); red_add(r, q3.z, p); red_add(r, q3.w, p);
+        scatter_one(r, q0.x, p, hacc); scatter_one(r, q0.y, p, hacc); scatter_one(r, q0.z, p, hacc); scatter_one(r, q0.w, p, hacc);
+        scatter_one(r, q1.x, p, hacc); scatter_one(r, q1.y, p, hacc); scatter_one(r, q1.z, p, hacc); scatter_one(r, q1.w, p, hacc);
+        scatter_one(r, q2.x, p, hacc); scatter_one(r, q2.y, p, hacc); scatter_one(r, q2.z, p, hacc); scatter_one(r, q2.w, p, hacc);
+        scatter_one(r, q3.x, p, hacc); scatter_one(r, q3.y, p, hacc); scatter_one(r, q3.z, p, hacc); scatter_one(r, q3.w, p, hacc);
     }
     for (; i < nbody; i += 32) {
         const int4 q = ld_edge4(body + i);
-        red_add(r, q.x, p); red_add(r, q.y, p); red_add(r, q.z, p); red_add(r, q.w, p);
+        scatter_one(r, q.x, p, hacc); scatter_one(r, q.y, p, hacc); scatter_one(r, q.z, p, hacc); scatter_one(r, q.w, p, hacc);
     }
     const unsigned tail = (deg - head) & 3u;
-    if (lane < (int)tail) red_add(r, ld_edge(nb + head + nbody * 4 + lane), p);
+    if (lane < (int)tail) scatter_one(r, ld_edge(nb + head + nbody * 4 + lane), p, hacc);
 }
 
 }  // namespace excent

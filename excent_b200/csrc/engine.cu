@@ -109,7 +109,29 @@ struct PushArgs {
     ull hub_cap;
     ull* hub_cnt;
     Ctrl* ctrl;
+    // hub-target aggregation: encoded cache entries name slots of hub_id[hub_k]
+    const int* hub_id;
+    int hub_k;
 };
+
+// Shared accumulators of the hub targets: zero at kernel start ...
+template <typename T>
+__device__ __forceinline__ T* hacc_init(int hub_k) {
+    extern __shared__ float4 s_dyn[];
+    T* h = reinterpret_cast<T*>(s_dyn);
+    for (int i = threadIdx.x; i < hub_k; i += blockDim.x) h[i] = T{};
+    __syncthreads();
+    return hub_k ? h : nullptr;
+}
+// ... and one reduction per nonzero slot at kernel end (after every warp finished).
+template <typename T>
+__device__ __forceinline__ void hacc_flush(T* h, T* r, const int* hub_id, int hub_k) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < hub_k; i += blockDim.x) {
+        const T v = h[i];
+        if (nonzero(v)) red_add(r, hub_id[i], v);
+    }
+}
 
 // ------------------------------------------------------------------ kernels
 
@@ -416,6 +438,7 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
     typedef typename Lane<L>::T T;
     T* x = reinterpret_cast<T*>(a.x);
     T* r = reinterpret_cast<T*>(a.r);
+    T* hacc = hacc_init<T>(a.hub_k);
     __shared__ const int* s_nb[BLOCK / 32][32];
     __shared__ unsigned s_ex[BLOCK / 32][32];
     __shared__ T s_p[BLOCK / 32][32];
@@ -458,38 +481,40 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
         // concatenated and lane j handles entry j of each 32-entry slice, UNROLL
         // slices at a time so each lane has UNROLL index loads in flight
         const unsigned ds = (act && !large) ? (unsigned)deg : 0u;
-        const unsigned incl = warp_incl_scan(ds, lane);
-        const unsigned tot = __shfl_sync(FULL, incl, 31);
-        if (tot) {
-            s_nb[wib][lane] = nb;
-            s_ex[wib][lane] = incl - ds;
-            if (ds) s_p[wib][lane] = p;
+        const unsigned nz = __ballot_sync(FULL, ds != 0);
+        if (nz) {
+            const unsigned incl = warp_incl_scan(ds, lane);
+            const unsigned tot = __shfl_sync(FULL, incl, 31);
+            const unsigned ex = incl - ds;
+            const int rank = __popc(nz & ((1u << lane) - 1u));
+            if (ds) { s_nb[wib][rank] = nb; s_ex[wib][rank] = ex; s_p[wib][rank] = p; }
             __syncwarp();
+            const unsigned le = lane == 31 ? FULL : (2u << lane) - 1u;
             for (unsigned j0 = 0; j0 < tot; j0 += 32 * UNROLL) {
                 int u[UNROLL];
                 int own[UNROLL];
 #pragma unroll
                 for (int k = 0; k < UNROLL; k++) {
-                    const unsigned j = j0 + 32 * k + lane;
-                    int lo = 0;
-#pragma unroll
-                    for (int step = 16; step > 0; step >>= 1) {
-                        const unsigned val = __shfl_sync(FULL, incl, lo + step - 1);
-                        if (val <= j) lo += step;
-                    }
-                    own[k] = j < tot ? lo : -1;
-                    u[k] = j < tot ? ld_edge(s_nb[wib][lo] + (j - s_ex[wib][lo])) : 0;
+                    // owner of entry wb+lane: the last nonempty list starting at or before it
+                    // (bit i of `starts`: a list begins at entry wb+i)
+                    const unsigned wb = j0 + 32 * k;
+                    const unsigned j = wb + lane;
+                    const unsigned starts =
+                        __reduce_or_sync(FULL, (ds && ex >= wb && ex - wb < 32) ? 1u << (ex - wb) : 0u);
+                    const int o = __popc(__ballot_sync(FULL, ds && ex <= wb)) - 1 + __popc(starts & le & ~1u);
+                    own[k] = j < tot ? o : -1;
+                    u[k] = j < tot ? ld_edge(s_nb[wib][o] + (j - s_ex[wib][o])) : 0;
                 }
 #pragma unroll
                 for (int k = 0; k < UNROLL; k++)
-                    if (own[k] >= 0) red_add(r, u[k], s_p[wib][own[k]]);
+                    if (own[k] >= 0) scatter_one(r, u[k], s_p[wib][own[k]], hacc);
             }
             __syncwarp();
         }
     }
     pushed = warp_sum(pushed);
     if (lane == 0) s_pushed[wib] = pushed;
-    __syncthreads();
+    hacc_flush(hacc, r, a.hub_id, a.hub_k);
     if (threadIdx.x == 0) {
         ull t = 0;
         for (int i = 0; i < BLOCK / 32; i++) t += s_pushed[i];
@@ -499,9 +524,11 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
 
 // Hub segments queued by k_push: one warp per 2048-entry segment.
 template <int L>
-__global__ void __launch_bounds__(BLOCK) k_hub(void* rv, const HubSeg* q, const ull* hub_cnt, ull cap) {
+__global__ void __launch_bounds__(BLOCK) k_hub(void* rv, const HubSeg* q, const ull* hub_cnt, ull cap,
+                                               const int* hub_id, int hub_k) {
     typedef typename Lane<L>::T T;
     T* r = reinterpret_cast<T*>(rv);
+    T* hacc = hacc_init<T>(hub_k);
     const int lane = threadIdx.x & 31;
     const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -511,8 +538,9 @@ __global__ void __launch_bounds__(BLOCK) k_hub(void* rv, const HubSeg* q, const 
         const HubSeg h = q[s];
         T p;
         if constexpr (L == 1) p = h.p.x; else p = h.p;
-        warp_scatter(r, h.nb, h.len, p, lane);
+        warp_scatter(r, h.nb, h.len, p, lane, hacc);
     }
+    hacc_flush(hacc, r, hub_id, hub_k);
 }
 
 // ---------------------------------------------------------------- pull pass
@@ -584,7 +612,8 @@ template <> __device__ __forceinline__ float4 zero_of<float4>() { return make_fl
 
 template <int L>
 __global__ void __launch_bounds__(BLOCK) k_pull(int n, void* rv, const void* Pv, const ull* idx, const int* cache,
-                                                HubSeg* hubq, ull* hub_cnt, ull hub_cap, Ctrl* ctrl) {
+                                                HubSeg* hubq, ull* hub_cnt, ull hub_cap, Ctrl* ctrl,
+                                                const int* hub_id) {
     typedef typename Lane<L>::T T;
     if (!ctrl->pull) return;
     T* r = reinterpret_cast<T*>(rv);
@@ -618,46 +647,55 @@ __global__ void __launch_bounds__(BLOCK) k_pull(int n, void* rv, const void* Pv,
             }
         }
         const unsigned ds = large ? 0u : (unsigned)deg;
+        const unsigned nz = __ballot_sync(FULL, ds != 0);
+        if (!nz) continue;
+        // the tile's nonempty lists in lane order, indexed by their rank among them
+        const int rank = __popc(nz & ((1u << lane) - 1u));
         const unsigned incl = warp_incl_scan(ds, lane);
         const unsigned tot = __shfl_sync(FULL, incl, 31);
-        if (!tot) continue;
-        s_nb[wib][lane] = nb;
-        s_ex[wib][lane] = incl - ds;
-        s_acc[wib][lane] = zero_of<T>();
+        const unsigned ex = incl - ds;
+        if (ds) { s_nb[wib][rank] = nb; s_ex[wib][rank] = ex; s_acc[wib][rank] = zero_of<T>(); }
         __syncwarp();
+        const unsigned le = lane == 31 ? FULL : (2u << lane) - 1u;   // lanes <= this one
         for (unsigned j0 = 0; j0 < tot; j0 += 32 * UNROLL) {
             T val[UNROLL];
-            int own[UNROLL];
+            int own[UNROLL], dist[UNROLL];
+            bool last[UNROLL];
 #pragma unroll
             for (int k = 0; k < UNROLL; k++) {
-                const unsigned j = j0 + 32 * k + lane;
-                int lo = 0;
-#pragma unroll
-                for (int step = 16; step > 0; step >>= 1) {
-                    const unsigned vl = __shfl_sync(FULL, incl, lo + step - 1);
-                    if (vl <= j) lo += step;
-                }
-                own[k] = j < tot ? lo : -1;
+                // window [wb, wb+32) of the concatenated lists: bit i of `starts` marks a list
+                // beginning at entry wb+i; the owner of entry wb is the last list starting at or
+                // before it, so lane i's owner is that one plus the starts in (wb, wb+i].
+                const unsigned wb = j0 + 32 * k;
+                const unsigned j = wb + lane;
+                const unsigned starts = __reduce_or_sync(FULL, (ds && ex >= wb && ex - wb < 32) ? 1u << (ex - wb) : 0u);
+                const int o0 = __popc(__ballot_sync(FULL, ds && ex <= wb)) - 1;
+                const unsigned sl = starts & le;
+                own[k] = o0 + __popc(sl & ~1u);
+                dist[k] = sl ? lane - (31 - __clz(sl)) : lane;
+                last[k] = j < tot && (lane == 31 || j + 1 == tot || ((starts >> (lane + 1)) & 1u));
                 val[k] = zero_of<T>();
-                if (j < tot) val[k] = P[ld_edge(s_nb[wib][lo] + (j - s_ex[wib][lo]))];
+                if (j < tot) {
+                    int u = ld_edge(s_nb[wib][own[k]] + (j - s_ex[wib][own[k]]));
+                    if (u < 0) u = hub_id[u & HUB_MASK];
+                    val[k] = __ldg(P + u);
+                }
             }
 #pragma unroll
             for (int k = 0; k < UNROLL; k++) {
-                // segmented inclusive sum over lanes with the same owner (owners ascend with the lane)
+                // segmented inclusive sum: lane i adds the lanes of its own list below it
                 T sv = val[k];
 #pragma unroll
                 for (int d = 1; d < 32; d <<= 1) {
                     const T t = shfl_up(sv, d);
-                    const int od = __shfl_up_sync(FULL, own[k], d);
-                    if (lane >= d && od == own[k]) acc_add(sv, t);
+                    if (d <= dist[k]) acc_add(sv, t);
                 }
-                const int nxt = __shfl_down_sync(FULL, own[k], 1);
-                if (own[k] >= 0 && (lane == 31 || nxt != own[k])) acc_add(s_acc[wib][own[k]], sv);
+                if (last[k]) acc_add(s_acc[wib][own[k]], sv);
                 __syncwarp();
             }
         }
         if (ds) {
-            const T add = s_acc[wib][lane];
+            const T add = s_acc[wib][rank];
             if (nonzero(add)) {
                 T cur = r[v];
                 acc_add(cur, add);
@@ -670,7 +708,7 @@ __global__ void __launch_bounds__(BLOCK) k_pull(int n, void* rv, const void* Pv,
 
 template <int L>
 __global__ void __launch_bounds__(BLOCK) k_pullhub(void* rv, const void* Pv, const HubSeg* q, const ull* hub_cnt,
-                                                   ull cap, const Ctrl* ctrl) {
+                                                   ull cap, const Ctrl* ctrl, const int* hub_id) {
     typedef typename Lane<L>::T T;
     if (!ctrl->pull) return;
     T* r = reinterpret_cast<T*>(rv);
@@ -686,16 +724,17 @@ __global__ void __launch_bounds__(BLOCK) k_pullhub(void* rv, const void* Pv, con
         const unsigned mis = (unsigned)(((uintptr_t)h.nb >> 2) & 3u);
         unsigned head = (4u - mis) & 3u;
         if (head > h.len) head = h.len;
-        if (lane < (int)head) acc_add(acc, P[ld_edge(h.nb + lane)]);
+        auto dec = [&](int u) { return u < 0 ? hub_id[u & HUB_MASK] : u; };
+        if (lane < (int)head) acc_add(acc, P[dec(ld_edge(h.nb + lane))]);
         const int4* body = reinterpret_cast<const int4*>(h.nb + head);
         const unsigned nbody = (h.len - head) >> 2;
         for (unsigned i = lane; i < nbody; i += 32) {
             const int4 e = ld_edge4(body + i);
-            const T a0 = P[e.x], a1 = P[e.y], a2 = P[e.z], a3 = P[e.w];
+            const T a0 = P[dec(e.x)], a1 = P[dec(e.y)], a2 = P[dec(e.z)], a3 = P[dec(e.w)];
             acc_add(acc, a0); acc_add(acc, a1); acc_add(acc, a2); acc_add(acc, a3);
         }
         const unsigned tail = (h.len - head) & 3u;
-        if (lane < (int)tail) acc_add(acc, P[ld_edge(h.nb + head + nbody * 4 + lane)]);
+        if (lane < (int)tail) acc_add(acc, P[dec(ld_edge(h.nb + head + nbody * 4 + lane))]);
         acc = warp_sum(acc);
         if (lane == 0 && nonzero(acc)) red_add(r, (int)h.pad, acc);
     }
@@ -736,6 +775,24 @@ __global__ void k_fill_hot(int lo, int hi, const int* hids, const ull* hoff, con
     const int* from = src + (idx[hids[w]] - e0);
     int* to = hedges + hoff[w];
     for (ull i = lane, d = hoff[w + 1] - hoff[w]; i < d; i += 32) to[i] = from[i];
+}
+
+
+// Encode / decode the edge cache for hub-target aggregation.
+__global__ void k_hub_encode(ull m, int* adj, const int* slot_of) {
+    for (ull e = blockIdx.x * (ull)blockDim.x + threadIdx.x; e < m; e += (ull)gridDim.x * blockDim.x) {
+        const int u = adj[e];
+        if (u >= 0) {
+            const int sl = slot_of[u];
+            if (sl >= 0) adj[e] = (int)(0x80000000u | (unsigned)sl);
+        }
+    }
+}
+__global__ void k_hub_decode(ull m, int* adj, const int* hub_id) {
+    for (ull e = blockIdx.x * (ull)blockDim.x + threadIdx.x; e < m; e += (ull)gridDim.x * blockDim.x) {
+        const int u = adj[e];
+        if (u < 0) adj[e] = hub_id[u & HUB_MASK];
+    }
 }
 
 // Measure i of a float4 layout into a float array, for readback.
@@ -802,6 +859,8 @@ struct excent_engine {
     float* d_tmp = nullptr;  // n floats for readback of the float4 layout
     float* d_v1 = nullptr;   // unit principal eigenvector for the EV normalisation step
     void* d_P = nullptr;     // per-vertex push weights of a pull pass
+    int* d_hub_id = nullptr; // hub-target aggregation: vertex of each slot
+    int hub_k = 0;           // slots in use (0: off)
     double pull_frac = 0;    // pull when the pending demand >= pull_frac * m (0: never)
     bool ev_proj = false;
     int ev_index = -1;
@@ -851,7 +910,7 @@ static int free_engine(excent_engine* e) {
     cudaDeviceSynchronize();
     if (e->gexec) cudaGraphExecDestroy(e->gexec);
     if (e->graph) cudaGraphDestroy(e->graph);
-    void* dptrs[] = {e->d_P, e->d_v1, e->d_idx, e->d_x, e->d_r, e->d_bitmap, e->d_cnt, e->d_cv0, e->d_list, e->d_ctrl, e->d_cmode,
+    void* dptrs[] = {e->d_hub_id, e->d_P, e->d_v1, e->d_idx, e->d_x, e->d_r, e->d_bitmap, e->d_cnt, e->d_cv0, e->d_list, e->d_ctrl, e->d_cmode,
                      e->d_wt_type, e->d_wt_prefix, e->d_hubq[0], e->d_hubq[1], e->d_hubq[2], e->d_hubcnt, e->d_log, e->d_trace, e->d_tmp, e->d_cache,
                      e->d_hids, e->d_hoff, e->d_hedges, e->d_hot, e->d_hlist};
     for (void* p : dptrs) if (p) cudaFree(p);
@@ -949,6 +1008,10 @@ static int engine_setup(excent_engine* e, int device, int n, ull m, const excent
     return EXCENT_OK;
 }
 
+static size_t hub_smem(const excent_engine* e) {
+    return (size_t)e->hub_k * (e->L == 1 ? sizeof(float) : sizeof(float4));
+}
+
 extern "C" int excent_measures_make(excent_measures* out, const char* measure, double alpha, double beta,
                                     double lambda, double eps_pr, double eps_katz, double eps_ev) {
     EX_CHECK_ARG(out && measure, "null argument");
@@ -1026,6 +1089,7 @@ extern "C" int excent_engine_reserve_cache(excent_engine* e, unsigned long long 
     invalidate_graph(e);
     EX_CUDA(cudaDeviceSynchronize());
     if (e->d_cache) { cudaFree(e->d_cache); e->d_cache = nullptr; e->cache_edges = 0; }
+    e->hub_k = 0;   // a fresh cache holds plain ids
     if (edges == 0) return EXCENT_OK;
     if (cudaMalloc((void**)&e->d_cache, edges * sizeof(int)) != cudaSuccess) {
         cudaGetLastError();
@@ -1180,17 +1244,18 @@ static PushArgs push_args(excent_engine* e, int q) {
     a.cache = e->d_cache;
     a.hids = e->d_hids; a.hoff = e->d_hoff; a.hedges = e->d_hedges; a.hlist = e->d_hlist;
     a.hubq = e->d_hubq[q]; a.hub_cap = e->hub_cap[q]; a.hub_cnt = e->d_hubcnt + q; a.ctrl = e->d_ctrl;
+    a.hub_id = e->d_hub_id; a.hub_k = e->hub_k;
     return a;
 }
 
 template <int SRC>
 static void launch_push(excent_engine* e, const PushArgs& a, int grid, cudaStream_t st) {
     if (e->L == 1) {
-        k_push<1, SRC><<<grid, BLOCK, 0, st>>>(a);
-        k_hub<1><<<e->grid_push, BLOCK, 0, st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap);
+        k_push<1, SRC><<<grid, BLOCK, hub_smem(e), st>>>(a);
+        k_hub<1><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
     } else {
-        k_push<4, SRC><<<grid, BLOCK, 0, st>>>(a);
-        k_hub<4><<<e->grid_push, BLOCK, 0, st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap);
+        k_push<4, SRC><<<grid, BLOCK, hub_smem(e), st>>>(a);
+        k_hub<4><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
     }
     e->launches += 2;
 }
@@ -1418,28 +1483,28 @@ static void enqueue_pass(excent_engine* e, double list_frac, int max_passes, cud
     if (ev) cudaEventRecord(ev[2], st);
     PushArgs a = push_args(e, 0);
     const int gt = e->sms * 8;
-    if (e->L == 1) k_push<1, SRC_TABLE><<<e->grid_push, BLOCK, 0, st>>>(a);
-    else k_push<4, SRC_TABLE><<<e->grid_push, BLOCK, 0, st>>>(a);
+    if (e->L == 1) k_push<1, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
+    else k_push<4, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
     e->launches++;
     if (pull_edges > 0) {   // each of these returns at once unless k_plan chose a pull pass
         if (e->L == 1) {
             k_take<1><<<gt, BLOCK, 0, st>>>(e->n, e->d_x, e->d_r, e->d_P, e->d_idx, e->M, e->d_ctrl);
             k_pull<1><<<e->grid_push, BLOCK, 0, st>>>(e->n, e->d_r, e->d_P, e->d_idx, e->d_cache, a.hubq, a.hub_cnt,
-                                                       a.hub_cap, e->d_ctrl);
+                                                       a.hub_cap, e->d_ctrl, e->d_hub_id);
         } else {
             k_take<4><<<gt, BLOCK, 0, st>>>(e->n, e->d_x, e->d_r, e->d_P, e->d_idx, e->M, e->d_ctrl);
             k_pull<4><<<e->grid_push, BLOCK, 0, st>>>(e->n, e->d_r, e->d_P, e->d_idx, e->d_cache, a.hubq, a.hub_cnt,
-                                                       a.hub_cap, e->d_ctrl);
+                                                       a.hub_cap, e->d_ctrl, e->d_hub_id);
         }
         e->launches += 2;
     }
     if (ev) cudaEventRecord(ev[3], st);
-    if (e->L == 1) k_hub<1><<<e->grid_push, BLOCK, 0, st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap);
-    else k_hub<4><<<e->grid_push, BLOCK, 0, st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap);
+    if (e->L == 1) k_hub<1><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
+    else k_hub<4><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
     e->launches++;
     if (pull_edges > 0) {
-        if (e->L == 1) k_pullhub<1><<<e->grid_push, BLOCK, 0, st>>>(e->d_r, e->d_P, a.hubq, a.hub_cnt, a.hub_cap, e->d_ctrl);
-        else k_pullhub<4><<<e->grid_push, BLOCK, 0, st>>>(e->d_r, e->d_P, a.hubq, a.hub_cnt, a.hub_cap, e->d_ctrl);
+        if (e->L == 1) k_pullhub<1><<<e->grid_push, BLOCK, 0, st>>>(e->d_r, e->d_P, a.hubq, a.hub_cnt, a.hub_cap, e->d_ctrl, e->d_hub_id);
+        else k_pullhub<4><<<e->grid_push, BLOCK, 0, st>>>(e->d_r, e->d_P, a.hubq, a.hub_cnt, a.hub_cap, e->d_ctrl, e->d_hub_id);
         e->launches++;
     }
     if (ev) cudaEventRecord(ev[4], st);
@@ -1633,6 +1698,57 @@ extern "C" int excent_device_info(int device, excent_device_info_t* out) {
     EX_CUDA(cudaDeviceGetAttribute(&out->sms, cudaDevAttrMultiProcessorCount, device));
     EX_CUDA(cudaDeviceGetAttribute(&out->cc_major, cudaDevAttrComputeCapabilityMajor, device));
     EX_CUDA(cudaDeviceGetAttribute(&out->cc_minor, cudaDevAttrComputeCapabilityMinor, device));
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_set_hub_targets(excent_engine* e, int k) {
+    EX_CHECK_ARG(e && k >= 0, "bad argument");
+    const int kmax = e->L == 1 ? 8192 : 2048;   // 32 KiB of shared accumulators per block
+    EX_CHECK_ARG(k <= kmax, "at most %d hub targets for this layout", kmax);
+    EX_CHECK_ARG(k <= e->n, "more hub targets than vertices");
+    EX_CUDA(cudaSetDevice(e->dev));
+    EX_CUDA(cudaDeviceSynchronize());
+    invalidate_graph(e);
+    if (e->hub_k && e->d_cache && e->cache_edges) {   // back to plain ids first
+        k_hub_decode<<<e->sms * 8, BLOCK, 0, e->s_main>>>(e->cache_edges, e->d_cache, e->d_hub_id);
+        e->launches++;
+        EX_CUDA(cudaStreamSynchronize(e->s_main));
+    }
+    e->hub_k = 0;
+    if (k > 0) {
+        EX_CHECK_ARG(e->d_cache && e->cache_edges, "load the edge cache before choosing hub targets");
+        std::vector<ull> idx((size_t)e->n + 1);
+        EX_CUDA(cudaMemcpy(idx.data(), e->d_idx, idx.size() * sizeof(ull), cudaMemcpyDeviceToHost));
+        std::vector<int> ids(e->n);
+        for (int v = 0; v < e->n; v++) ids[v] = v;
+        auto deg = [&](int v) { return idx[v + 1] - idx[v]; };
+        std::nth_element(ids.begin(), ids.begin() + (k - 1), ids.end(), [&](int a, int b) {
+            return deg(a) > deg(b) || (deg(a) == deg(b) && a < b);
+        });
+        ids.resize(k);
+        std::sort(ids.begin(), ids.end());
+        std::vector<int> slot_of(e->n, -1);
+        for (int i = 0; i < k; i++) slot_of[ids[i]] = i;
+        if (!e->d_hub_id) EX_ALLOC(e->d_hub_id, (size_t)kmax * sizeof(int));
+        int* d_slot = nullptr;
+        EX_ALLOC(d_slot, (size_t)e->n * sizeof(int));
+        cudaError_t err = cudaMemcpy(e->d_hub_id, ids.data(), (size_t)k * sizeof(int), cudaMemcpyHostToDevice);
+        if (err == cudaSuccess)
+            err = cudaMemcpy(d_slot, slot_of.data(), (size_t)e->n * sizeof(int), cudaMemcpyHostToDevice);
+        if (err == cudaSuccess) {
+            k_hub_encode<<<e->sms * 8, BLOCK, 0, e->s_main>>>(e->cache_edges, e->d_cache, d_slot);
+            e->launches++;
+            err = cudaStreamSynchronize(e->s_main);
+        }
+        cudaFree(d_slot);
+        EX_CUDA(err);
+        e->hub_k = k;
+    }
+    const size_t smem = hub_smem(e);
+    int occ = 0;
+    if (e->L == 1) EX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_push<1, SRC_TABLE>, BLOCK, smem));
+    else EX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_push<4, SRC_TABLE>, BLOCK, smem));
+    e->grid_push = e->sms * std::max(1, occ);
     return EXCENT_OK;
 }
 

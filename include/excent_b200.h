@@ -214,6 +214,16 @@ int excent_engine_write(excent_engine* e, int i, const float* x, const float* r)
 int excent_engine_trace(excent_engine* e, int enable);
 int excent_engine_read_trace(excent_engine* e, uint16_t* out);
 
+/* Hub-target aggregation: re-encode the entries of the k highest-degree
+ * vertices in the HBM edge cache as slots, so push kernels sum the
+ * contributions to those targets in shared memory and add them to the
+ * residuals once per block instead of once per entry (the hubs of a power-law
+ * graph receive a large share of all entries, and same-address reductions
+ * serialise in L2). k <= 8192 (one measure) or 2048 (float4 layout); 0 turns
+ * it off and restores plain ids. Call after the cache is loaded; reloading
+ * the cache turns it off. No reference counterpart. */
+int excent_engine_set_hub_targets(excent_engine* e, int k);
+
 /* Direction-optimised passes for the device solve on a SYMMETRIC graph (every
  * edge stored in both directions): a pass whose pending demand (sum of
  * pending degrees) is at least pull_frac * m runs as a gather. It takes every

@@ -323,3 +323,37 @@ def test_pull_passes_match_push(rmat16, measure, use_graph):
     for k in names:
         print(k, "push", res[(0.0, k)], "pull", res[(0.3, k)])
         assert res[(0.3, k)]["l1_rel"] <= 1.1 * res[(0.0, k)]["l1_rel"] + 1e-7
+
+
+@pytest.mark.parametrize("measure", ["pr", "all"])
+@pytest.mark.parametrize("k", [1, 64, 2048])
+@pytest.mark.parametrize("pull", [0.0, 0.3])
+def test_hub_targets_match_plain_push(rmat16, measure, k, pull):
+    """Shared-memory aggregation of the top-k targets reaches the same fixed
+    point, leaves the cache decodable (set to 0 restores the plain ids) and
+    works with gather passes reading the encoded cache."""
+    n, idx, adj = rmat16
+    par = O.params(n, idx, adj)
+    kw = dict(alpha=0.9 / par["_lambda"], lam=par["_lambda"], eps_katz=1e-5, eps_ev=1e-5) if measure == "all" else {}
+    names = ["pr", "katz", "ev"] if measure == "all" else ["pr"]
+    res = {}
+    for hk in (0, k):
+        meas = X.measures(measure, **kw)
+        eng = make_engine(n, idx, adj, meas)
+        eng.set_pull(pull)
+        eng.set_hub_targets(hk)
+        eng.solve()
+        for i, name in enumerate(names):
+            r = eng.read(i, residual=True)
+            assert np.all(np.abs(r) <= np.float32(meas.eps[i]))
+            ref = O.reference_solution(n, idx, adj, name, alpha=kw.get("alpha"))
+            res[(hk, name)] = O.compare(name, ref, eng.read(i))
+        if hk:   # back to plain ids: a second solve from scratch still matches
+            eng.set_hub_targets(0)
+            eng.solve()
+            c = O.compare(names[0], O.reference_solution(n, idx, adj, names[0], alpha=kw.get("alpha")), eng.read(0))
+            assert c["l1_rel"] <= 1.1 * res[(0, names[0])]["l1_rel"] + 1e-7
+        eng.close()
+    for name in names:
+        assert res[(k, name)]["l1_rel"] <= 1.1 * res[(0, name)]["l1_rel"] + 1e-7, (name, res)
+        assert res[(k, name)]["top100"] >= 95
