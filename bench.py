@@ -42,6 +42,7 @@ CONFIGS = {
     "pr16": (16, 16, 1, "pr"),
     "ppr256": (24, 16, 2, "ppr"),
     "adjoint22": (22, 16, 4, "adjoint"),
+    "ooc28": (28, 32, 3, "ooc"),
 }
 
 
@@ -72,6 +73,11 @@ def parse():
     ap.add_argument("--ref-gpu", action="store_true",
                     help="also run this repo's CLI and the reference CLI (built from source) on the same EGR file")
     ap.add_argument("--ref-passes", type=int, default=200, help="pass cap of the CLI runs for 'all'")
+    ap.add_argument("--ooc-budget-gb", type=float, default=16.0,
+                    help="device memory left to the CLIs in the out-of-core run (the rest is held as ballast)")
+    ap.add_argument("--ooc-dir", default=None, help="directory for the out-of-core EGR file (default: temp dir)")
+    ap.add_argument("--ooc-measures", default="pr", help="comma-separated measures of the out-of-core run")
+    ap.add_argument("--ooc-ref", default="on", choices=["on", "off"], help="also run the reference CLI out of core")
     ap.add_argument("--hub-targets", type=int, default=0,
                     help="shared-memory aggregation of the k highest-degree targets (0: off)")
     ap.add_argument("--ev-init", default="fp64", choices=["fp64", "reference"],
@@ -539,6 +545,150 @@ def cli_compare(a, idx, adj, measure, meas, lam, device):
         shutil.rmtree(d, ignore_errors=True)
 
 
+def parse_cli(out):
+    """Figures of one CLI run, from the stdout lines both CLIs print (src/excent.cu:756-804)."""
+    import re
+    f = {"passes": int(re.search(r"^passes (\d+)", out, re.M).group(1)),
+         "pushed_x_m": float(re.search(r"edges pushed: ([0-9.]+) x", out).group(1)),
+         "passes_s": float(re.search(r"time: .* passes ([0-9.]+)s", out).group(1))}
+    mb = re.search(r"bytes shipped: stream ([0-9.]+) GB, gather ([0-9.]+) GB", out)
+    f["stream_gb"], f["gather_gb"] = float(mb.group(1)), float(mb.group(2))
+    mf = re.search(r"page faults in passes: major (\d+), minor (\d+)", out)
+    f["major_faults"] = int(mf.group(1))
+    f["gather_passes"] = len(re.findall(r"^pass +\d+:.*gather [1-9]", out, re.M))
+    mt = re.search(r"fetch rule: tau = ([0-9.]+)", out)
+    f["tau"] = float(mt.group(1)) if mt else None
+    mw = re.search(r"gpu wait ([0-9.]+)s", out)
+    f["gpu_wait_s"] = float(mw.group(1)) if mw else None
+    mi = re.search(r"cpu io ([0-9.]+)s", out)
+    f["cpu_io_s"] = float(mi.group(1)) if mi else None
+    return f
+
+
+def evict(path):
+    """Drop the file's pages from the host page cache (what the reference's evict_file does)."""
+    fd = os.open(path, os.O_RDONLY)
+    try:
+        os.fsync(fd)
+        os.posix_fadvise(fd, 0, 0, os.POSIX_FADV_DONTNEED)
+    finally:
+        os.close(fd)
+
+
+def h2d_gbs(torch, nbytes=1 << 30, reps=5):
+    """Pinned host -> device copy bandwidth on this box (the host-link denominator)."""
+    h = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    d = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    d.copy_(h, non_blocking=True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        d.copy_(h, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    bw = nbytes * reps / (e0.elapsed_time(e1) / 1e3) / 1e9
+    del h, d
+    torch.cuda.empty_cache()
+    return bw
+
+
+def run_ooc(a, world, rank, local, dist):
+    """Out-of-core PageRank (and eigenvector) through the CLI on an EGR file larger than the
+    device memory left to it, page cache evicted before each run; this repo's CLI against the
+    reference CLI on the same file, flags and device memory."""
+    import shutil
+    import subprocess
+    import tempfile
+
+    import torch
+
+    import excent_b200 as X
+    import excent_b200._capi as K
+    torch.cuda.set_device(local)
+    scale, ef, seed, _ = CONFIGS[a.config]
+    scale = a.scale or scale
+    n = 1 << scale
+    est = 16 + 8 * (n + 1) + 4 * n * ef   # upper bound of the file size
+    base = a.ooc_dir or tempfile.gettempdir()
+    free_disk = shutil.disk_usage(base).free
+    if free_disk < est * 1.05:
+        return {"metric": "GTEPS (out of core)", "unavailable": f"needs {est / 1e9:.1f} GB of disk in {base}, "
+                f"{free_disk / 1e9:.1f} GB free"}
+    d = tempfile.mkdtemp(prefix="excent_ooc_", dir=base)
+    try:
+        path = os.path.join(d, f"rmat{scale}.egr")
+        t0 = time.perf_counter()
+        m, parts = X.rmat_write_egr(path, scale, ef, seed, device=local)
+        t_gen = time.perf_counter() - t0
+        log(f"wrote {path}: n={n} m={m} in {parts} partitions, {t_gen:.1f}s")
+        torch.cuda.synchronize()
+        link = h2d_gbs(torch)
+        log(f"pinned H2D {link:.1f} GB/s")
+        free, total = torch.cuda.mem_get_info()
+        keep = int(a.ooc_budget_gb * 1e9)
+        ballast = None
+        if free > keep:
+            ballast = torch.empty(free - keep, dtype=torch.uint8, device="cuda")
+        free2, _ = torch.cuda.mem_get_info()
+        log(f"device memory left to the CLIs: {free2 / 1e9:.2f} GB")
+        home = os.path.join(d, "home")
+        os.makedirs(home, exist_ok=True)
+        env = dict(os.environ, HOME=home)
+        ref_bin = os.path.join(ROOT, "oracle", "_ref", "excent")
+        runs = {}
+        for measure in a.ooc_measures.split(","):
+            args = [path, "--measure", measure, "--count-pushes"]
+            if measure in ("ev", "all", "katz"):
+                return {"metric": "GTEPS (out of core)", "unavailable": "eigenvector/Katz constants need the "
+                        "FP64 lambda1 of the full graph, not computed out of core here"}
+            arms = [("ours", K.CLI_PATH)]
+            if a.ooc_ref == "on" and os.path.exists(ref_bin):
+                arms.append(("reference", ref_bin))
+            for name, binary in arms:
+                evict(path)
+                w0 = time.perf_counter()
+                r = subprocess.run([binary, *args], capture_output=True, text=True, env=env, timeout=3600)
+                wall = time.perf_counter() - w0
+                if r.returncode != 0:
+                    runs[f"{measure}/{name}"] = {"error": (r.stderr or r.stdout)[-400:]}
+                    continue
+                f = parse_cli(r.stdout)
+                f["wall_s"] = round(wall, 2)
+                b_link = (f["stream_gb"] + f["gather_gb"]) * 1e9 + f["gather_passes"] * n / 8
+                f["link_bytes"] = int(b_link)
+                f["link_bound_s"] = round(b_link / (link * 1e9), 3)
+                f["frac_of_link_bound"] = round(f["link_bound_s"] / f["passes_s"], 4) if f["passes_s"] else None
+                f["gteps"] = round(f["pushed_x_m"] * m / f["passes_s"] / 1e9, 4) if f["passes_s"] else None
+                runs[f"{measure}/{name}"] = f
+                log(f"{measure}/{name}: {f}")
+                with open(os.path.join(ROOT, "gpurun_out", f"ooc_{measure}_{name}.log") if os.path.isdir(
+                        os.path.join(ROOT, "gpurun_out")) else os.devnull, "w") as fo:
+                    fo.write(r.stdout)
+        del ballast
+        ours = runs.get(f"{a.ooc_measures.split(',')[0]}/ours", {})
+        if "passes_s" not in ours:
+            return {"metric": "GTEPS (out of core)", "unavailable": f"CLI run failed: {ours}"}
+        return {
+            "metric": "GTEPS (adjacency entries pushed per second, out of core, solve to eps)",
+            "value": ours["gteps"], "unit": "GTEPS", "n_gpus": world, "steps": 1, "warmup": 0,
+            "ms_per_step": round(ours["passes_s"] * 1e3, 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded R-MAT written as EGR on local disk)",
+            "config": {"workload": f"{a.ooc_measures} out of core on R-MAT scale {scale} EF {ef} seed {seed}",
+                       "n": n, "m": m, "egr_gb": round(os.path.getsize(path) / 1e9, 2), "partitions": parts,
+                       "device_gb_left": round(free2 / 1e9, 2), "generation_s": round(t_gen, 1),
+                       "page_cache": "evicted before each CLI run", "l2_note": "inputs far larger than L2"},
+            "e2e": {"value": ours["gteps"], "unit": "GTEPS", "note": "the CLI from file to dumps is the end to end path",
+                    "h2d_bytes_per_step": ours["link_bytes"], "d2h_bytes_per_step": 4 * n},
+            "roofline": {"bound": "host-link", "achieved": round(ours["link_bytes"] / ours["passes_s"] / 1e9, 2),
+                         "peak": round(link, 2), "peak_source": "pinned H2D copy measured in this run", "unit": "GB/s",
+                         "frac": ours["frac_of_link_bound"], "traffic": None},
+            "runs": runs,
+        }
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
 def cpu_baseline(n, idx, adj, meas, measure, lam):
     pushed, passes, t = cpu_sample(n, idx, adj, meas, measure, lam, max_edges=len(adj))
     return {"value": round(pushed / t / 1e9, 5), "unit": "GTEPS", "cores": os.cpu_count(), "kind": "port",
@@ -553,6 +703,11 @@ def run_reference(a, world, rank):
     import oracle as O
     scale, ef, seed, measure = CONFIGS[a.config]
     scale = a.scale or scale
+    if measure not in ("pr", "all"):
+        why = {"ppr": "the reference has no batched personalized PageRank",
+               "adjoint": "the reference has no adjoint or gradient path",
+               "ooc": "the CPU port does not run out of core; the out-of-core run times the reference CLI beside ours"}
+        return {"impl": "reference", "unavailable": why[measure]}
     n, idx, adj = O.rmat_graph(scale, ef, seed, fast=True)
     lam = O.lambda1(n, idx, adj, 1e-10) if measure == "all" else None
     eps = [1e-2, 1e-6, 1e-6] if measure == "all" else [1e-2]
@@ -594,7 +749,7 @@ def main():
             print(json.dumps(res))
         return
     kind = CONFIGS[a.config][3]
-    runner = {"ppr": run_ppr, "adjoint": run_adjoint}.get(kind, run_ours)
+    runner = {"ppr": run_ppr, "adjoint": run_adjoint, "ooc": run_ooc}.get(kind, run_ours)
     res = runner(a, world, rank, local, dist)
     if dist:
         dist.barrier()

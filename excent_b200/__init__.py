@@ -12,6 +12,7 @@ generates seeded R-MAT graphs on the device.
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -267,6 +268,16 @@ def reference_fp64(n, d_idx, d_adj, measure, alpha=0.0, beta=1.0, tol=1e-9, maxi
     call("excent_reference_fp64", int(device), int(n), _ptr(d_idx), _ptr(d_adj), kind, float(alpha), float(beta),
          float(tol), int(maxit), _tp(x, _capi.f64p), C.byref(it))
     return x, it.value
+
+
+def rmat_write_egr(path, scale, edge_factor, seed, a=0.57, b=0.19, c=0.19, max_part_keys=0, device=0):
+    """The symmetric R-MAT graph of DeviceGraph, generated in source partitions that fit device
+    memory and written as a wide EGR file (excent_rmat_write_egr). Returns (m, partitions)."""
+    m = C.c_uint64()
+    parts = C.c_int()
+    call("excent_rmat_write_egr", int(device), int(scale), int(edge_factor), int(seed), a, b, c,
+         int(max_part_keys), os.fsencode(path), C.byref(m), C.byref(parts))
+    return m.value, parts.value
 
 
 class DeviceGraph:

@@ -125,6 +125,8 @@ PROTOS = [
     ("excent_cli_main", C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
     ("excent_rmat_generate", C.c_int, [C.c_int, C.c_int, C.c_int, u64, C.c_double, C.c_double, C.c_double,
                                        C.c_int, C.c_int, C.POINTER(vp)]),
+    ("excent_rmat_write_egr", C.c_int, [C.c_int, C.c_int, C.c_int, u64, C.c_double, C.c_double, C.c_double, u64,
+                                        C.c_char_p, u64p, C.POINTER(C.c_int)]),
     ("excent_dgraph_info", C.c_int, [vp, C.POINTER(C.c_int), u64p]),
     ("excent_dgraph_device_ptrs", C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
     ("excent_dgraph_download", C.c_int, [vp, vp, vp, vp]),

@@ -453,6 +453,15 @@ typedef struct excent_dgraph excent_dgraph;
  * reference ingests .mtx files (tools/efficient_converter.py:5-113). */
 int excent_rmat_generate(int device, int scale, int edge_factor, unsigned long long seed, double a, double b,
                          double c, int symmetric, int weights, excent_dgraph** out);
+/* The symmetric graph of excent_rmat_generate (the same CSR, bit for bit),
+ * generated in source-vertex partitions that fit device memory and written
+ * as a wide EGR file: for out-of-core graphs larger than HBM holds at once.
+ * max_part_keys = 0 sizes the partitions from free device memory. Writes the
+ * entry count to *m_out and the number of partitions to *parts_out. No
+ * reference counterpart (the reference converts .mtx files). */
+int excent_rmat_write_egr(int device, int scale, int edge_factor, unsigned long long seed, double a, double b,
+                          double c, unsigned long long max_part_keys, const char* path, unsigned long long* m_out,
+                          int* parts_out);
 int excent_dgraph_info(excent_dgraph* g, int* n, unsigned long long* m);
 int excent_dgraph_device_ptrs(excent_dgraph* g, unsigned long long** idx, int32_t** adj, float** w);
 /* Copy offsets (n+1), lists (m) and weights (m, if generated) to host memory; any may be NULL. */

@@ -244,6 +244,30 @@ def test_rmat_generator_bitexact_vs_oracle():
         g.close()
 
 
+@pytest.mark.parametrize("scale,ef,seed,part_keys", [(10, 16, 1, 0), (12, 8, 3, 9000), (14, 16, 5, 40000),
+                                                     (13, 32, 2, 1 << 40)])
+def test_partitioned_egr_writer_bitexact(tmp_path, scale, ef, seed, part_keys):
+    """The out-of-core generator writes the same graph as the one-shot device
+    generator and the oracle's CPU generator, whatever the partition size."""
+    p = str(tmp_path / "g.egr")
+    m, parts = X.rmat_write_egr(p, scale, ef, seed, max_part_keys=part_keys)
+    if part_keys and part_keys < 1 << 20:
+        assert parts > 1
+    n, idx, adj = O.read_egr(p)
+    n_o, idx_o, adj_o = O.rmat_graph(scale, ef, seed)
+    assert n == n_o and m == len(adj_o) == len(adj)
+    assert np.array_equal(idx, idx_o) and np.array_equal(adj, adj_o)
+    g = X.DeviceGraph(scale, ef, seed)
+    i2, a2, _ = g.download()
+    assert np.array_equal(i2, idx) and np.array_equal(a2[:g.m], adj)
+    g.close()
+
+
+def test_partitioned_egr_writer_rejects_tiny_partitions(tmp_path):
+    with pytest.raises(X.ExcentError, match="source bucket"):
+        X.rmat_write_egr(str(tmp_path / "g.egr"), 12, 16, 1, max_part_keys=10)
+
+
 @pytest.mark.parametrize("pull", [0.0, 0.3])
 @pytest.mark.parametrize("measure", ["pr", "katz", "ev", "all"])
 def test_error_no_looser_than_reference_engine(sample, measure, pull):
