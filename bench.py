@@ -78,6 +78,8 @@ def parse():
     ap.add_argument("--ooc-dir", default=None, help="directory for the out-of-core EGR file (default: temp dir)")
     ap.add_argument("--ooc-measures", default="pr", help="comma-separated measures of the out-of-core run")
     ap.add_argument("--ooc-ref", default="on", choices=["on", "off"], help="also run the reference CLI out of core")
+    ap.add_argument("--hub-first", default="off", choices=["on", "off"],
+                    help="push the high-degree lists first in every pass")
     ap.add_argument("--hub-targets", type=int, default=0,
                     help="shared-memory aggregation of the k highest-degree targets (0: off)")
     ap.add_argument("--ev-init", default="fp64", choices=["fp64", "reference"],
@@ -187,6 +189,7 @@ def run_ours(a, world, rank, local, dist):
         eng.ev_project(v1)
     eng.set_pull(a.pull_frac)
     eng.set_hub_targets(a.hub_targets)
+    eng.set_hub_order(a.hub_first == "on")
     use_graph = not a.no_graph
     for _ in range(a.warmup):
         s = eng.solve(use_graph=use_graph)
@@ -275,7 +278,8 @@ def run_ours(a, world, rank, local, dist):
                    "l2_note": "inputs larger than L2 (edge cache %.2f GB)" % (m * 4 / 1e9),
                    "cuda_graph": use_graph, "parallelism": f"{world} independent replicas",
                    "ev_init": a.ev_init, "ev_project": a.ev_project if measure == "all" else None,
-                   "pull_frac": a.pull_frac, "hub_targets": a.hub_targets},
+                   "pull_frac": a.pull_frac, "hub_targets": a.hub_targets,
+                   "hub_first": a.hub_first},
         "e2e": {"value": round(e_pushed / te / 1e9, 4), "unit": "GTEPS", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": round(te / a.steps * 1e3, 3),
                 "wall_ms_per_step": round(te_wall / a.steps * 1e3, 3)},

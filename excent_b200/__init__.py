@@ -206,6 +206,10 @@ class Engine:
         """Shared-memory aggregation of the contributions to the k highest-degree targets (0: off)."""
         call("excent_engine_set_hub_targets", self.h, int(k))
 
+    def set_hub_order(self, first=True):
+        """Device solve: push the lists longer than 256 entries first in every pass."""
+        call("excent_engine_set_hub_order", self.h, int(bool(first)))
+
     def set_pull(self, frac):
         """Gather passes when the pending demand >= frac * m (symmetric graphs only; 0 = never)."""
         call("excent_engine_set_pull", self.h, float(frac))

@@ -26,7 +26,7 @@ static constexpr unsigned HUB_SEG = 1024; // edges per hub segment
 static constexpr int UNROLL = 4;          // independent index loads per lane in flight
 static constexpr int BLOCK = 256;
 
-enum { SRC_TABLE = 0, SRC_CHUNK = 1, SRC_GATHER = 2, SRC_HOT = 3 };
+enum { SRC_TABLE = 0, SRC_CHUNK = 1, SRC_GATHER = 2, SRC_HOT = 3, SRC_HUBS = 4 };
 enum { WT_NONE = 0, WT_LIST = 1, WT_RANGE = 2 };
 
 struct HubSeg {
@@ -112,6 +112,11 @@ struct PushArgs {
     // hub-target aggregation: encoded cache entries name slots of hub_id[hub_k]
     const int* hub_id;
     int hub_k;
+    // high-degree-first order: SRC_HUBS pushes the lists longer than HUB_MIN
+    // (hubv[*hubv_cnt]) first; SRC_TABLE then skips them
+    const int* hubv;
+    const ull* hubv_cnt;
+    int hubs_first;
 };
 
 // Shared accumulators of the hub targets: zero at kernel start ...
@@ -406,6 +411,13 @@ __device__ __forceinline__ bool get_item(const PushArgs& a, long long t, int& v,
         deg = a.off[t + 1] - b;
         nb = a.gedges + b;
         return true;
+    } else if constexpr (SRC == SRC_HUBS) {
+        if (t >= (long long)*a.hubv_cnt) return false;
+        v = a.hubv[t];
+        const ull b = a.idx[v];
+        deg = a.idx[v + 1] - b;
+        nb = a.cache + b;
+        return true;
     } else {
         if (t >= (long long)a.ctrl->hcount) return false;
         const int j = a.hlist[t];
@@ -422,6 +434,7 @@ __device__ __forceinline__ long long item_total(const PushArgs& a) {
     if constexpr (SRC == SRC_TABLE) return a.wt_prefix[a.nc];
     else if constexpr (SRC == SRC_CHUNK) return a.ccount;
     else if constexpr (SRC == SRC_GATHER) return a.gk;
+    else if constexpr (SRC == SRC_HUBS) return a.ctrl->pull ? 0 : (long long)*a.hubv_cnt;
     else return a.ctrl->hcount;
 }
 
@@ -454,7 +467,8 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
         ull deg = 0;
         T p{};
         bool act = false;
-        if (get_item<SRC>(a, tile * 32 + lane, v, nb, deg)) {
+        if (get_item<SRC>(a, tile * 32 + lane, v, nb, deg) &&
+            !(SRC == SRC_TABLE && a.hubs_first && deg > HUB_MIN)) {   // pushed first by SRC_HUBS
             p = take(x, r, v, deg, a.M);
             act = nonzero(p) && deg > 0;
         }
@@ -538,6 +552,7 @@ __global__ void __launch_bounds__(BLOCK) k_hub(void* rv, const HubSeg* q, const 
         const HubSeg h = q[s];
         T p;
         if constexpr (L == 1) p = h.p.x; else p = h.p;
+        if (!nonzero(p)) continue;   // a gather pass's segment (k_pullhub sums it)
         warp_scatter(r, h.nb, h.len, p, lane, hacc);
     }
     hacc_flush(hacc, r, hub_id, hub_k);
@@ -778,6 +793,22 @@ __global__ void k_fill_hot(int lo, int hi, const int* hids, const ull* hoff, con
 }
 
 
+// Vertices whose lists are longer than HUB_MIN, appended in any order.
+__global__ void k_hub_list(int n, const ull* idx, int* out, ull* cnt) {
+    const int lane = threadIdx.x & 31;
+    for (long long v0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) & ~31ll; v0 < n;
+         v0 += (long long)gridDim.x * blockDim.x) {
+        const long long v = v0 + lane;
+        const bool h = v < n && idx[v + 1] - idx[v] > HUB_MIN;
+        const unsigned b = __ballot_sync(FULL, h);
+        if (!b) continue;
+        ull base = 0;
+        if (lane == 0) base = atomicAdd(cnt, (ull)__popc(b));
+        base = __shfl_sync(FULL, base, 0);
+        if (h) out[base + __popc(b & ((1u << lane) - 1u))] = (int)v;
+    }
+}
+
 // Encode / decode the edge cache for hub-target aggregation.
 __global__ void k_hub_encode(ull m, int* adj, const int* slot_of) {
     for (ull e = blockIdx.x * (ull)blockDim.x + threadIdx.x; e < m; e += (ull)gridDim.x * blockDim.x) {
@@ -860,7 +891,12 @@ struct excent_engine {
     float* d_v1 = nullptr;   // unit principal eigenvector for the EV normalisation step
     void* d_P = nullptr;     // per-vertex push weights of a pull pass
     int* d_hub_id = nullptr; // hub-target aggregation: vertex of each slot
+    int* d_slot = nullptr;   // slot of each vertex (-1: none), kept to encode later cache loads
     int hub_k = 0;           // slots in use (0: off)
+    int* d_hubv = nullptr;   // high-degree-first order: vertices with lists longer than HUB_MIN
+    ull* d_hubv_cnt = nullptr;
+    bool hubs_first = false;
+    bool hubv_stale = true;
     double pull_frac = 0;    // pull when the pending demand >= pull_frac * m (0: never)
     bool ev_proj = false;
     int ev_index = -1;
@@ -910,7 +946,7 @@ static int free_engine(excent_engine* e) {
     cudaDeviceSynchronize();
     if (e->gexec) cudaGraphExecDestroy(e->gexec);
     if (e->graph) cudaGraphDestroy(e->graph);
-    void* dptrs[] = {e->d_hub_id, e->d_P, e->d_v1, e->d_idx, e->d_x, e->d_r, e->d_bitmap, e->d_cnt, e->d_cv0, e->d_list, e->d_ctrl, e->d_cmode,
+    void* dptrs[] = {e->d_hub_id, e->d_slot, e->d_hubv, e->d_hubv_cnt, e->d_P, e->d_v1, e->d_idx, e->d_x, e->d_r, e->d_bitmap, e->d_cnt, e->d_cv0, e->d_list, e->d_ctrl, e->d_cmode,
                      e->d_wt_type, e->d_wt_prefix, e->d_hubq[0], e->d_hubq[1], e->d_hubq[2], e->d_hubcnt, e->d_log, e->d_trace, e->d_tmp, e->d_cache,
                      e->d_hids, e->d_hoff, e->d_hedges, e->d_hot, e->d_hlist};
     for (void* p : dptrs) if (p) cudaFree(p);
@@ -1008,6 +1044,13 @@ static int engine_setup(excent_engine* e, int device, int n, ull m, const excent
     return EXCENT_OK;
 }
 
+// Encode cache entries [e0, e1) for hub-target aggregation (no-op when off).
+static void hub_encode(excent_engine* e, ull e0, ull e1, cudaStream_t st) {
+    if (!e->hub_k || !e->d_slot || e1 <= e0) return;
+    k_hub_encode<<<e->sms * 8, BLOCK, 0, st>>>(e1 - e0, e->d_cache + e0, e->d_slot);
+    e->launches++;
+}
+
 static size_t hub_smem(const excent_engine* e) {
     return (size_t)e->hub_k * (e->L == 1 ? sizeof(float) : sizeof(float4));
 }
@@ -1069,6 +1112,7 @@ extern "C" int excent_engine_upload_offsets(excent_engine* e, const unsigned lon
     EX_CUDA(cudaSetDevice(e->dev));
     EX_CUDA(cudaMemcpyAsync(e->d_idx + v0, idx, count * sizeof(ull), cudaMemcpyHostToDevice, e->s_main));
     EX_CUDA(cudaStreamSynchronize(e->s_main));
+    e->hubv_stale = true;
     return EXCENT_OK;
 }
 
@@ -1078,7 +1122,10 @@ extern "C" int excent_engine_upload_device(excent_engine* e, const unsigned long
     EX_CUDA(cudaMemcpyAsync(e->d_idx, d_idx, ((size_t)e->n + 1) * sizeof(ull), cudaMemcpyDeviceToDevice, e->s_main));
     if (e->cache_edges != e->m) EX_TRY(excent_engine_reserve_cache(e, e->m));
     if (e->m) EX_CUDA(cudaMemcpyAsync(e->d_cache, d_adj, e->m * sizeof(int), cudaMemcpyDeviceToDevice, e->s_main));
+    hub_encode(e, 0, e->m, e->s_main);
     EX_CUDA(cudaStreamSynchronize(e->s_main));
+    EX_CUDA(cudaGetLastError());
+    e->hubv_stale = true;
     std::fill(e->loaded.begin(), e->loaded.end(), 1);
     return EXCENT_OK;
 }
@@ -1090,6 +1137,7 @@ extern "C" int excent_engine_reserve_cache(excent_engine* e, unsigned long long 
     EX_CUDA(cudaDeviceSynchronize());
     if (e->d_cache) { cudaFree(e->d_cache); e->d_cache = nullptr; e->cache_edges = 0; }
     e->hub_k = 0;   // a fresh cache holds plain ids
+    if (e->d_slot) { cudaFree(e->d_slot); e->d_slot = nullptr; }
     if (edges == 0) return EXCENT_OK;
     if (cudaMalloc((void**)&e->d_cache, edges * sizeof(int)) != cudaSuccess) {
         cudaGetLastError();
@@ -1106,7 +1154,9 @@ extern "C" int excent_engine_load_cache(excent_engine* e, unsigned long long e0,
     EX_CHECK_ARG(e && edges && e0 <= e1 && e1 <= e->cache_edges, "edges [%llu, %llu) outside the cache", e0, e1);
     EX_CUDA(cudaSetDevice(e->dev));
     EX_CUDA(cudaMemcpyAsync(e->d_cache + e0, edges, (e1 - e0) * sizeof(int), cudaMemcpyHostToDevice, e->s_main));
+    hub_encode(e, e0, e1, e->s_main);
     EX_CUDA(cudaStreamSynchronize(e->s_main));
+    EX_CUDA(cudaGetLastError());
     for (int c = 0; c < e->nc; c++) if (e->ce[c] >= e0 && e->ce[c + 1] <= e1) e->loaded[c] = 1;
     return EXCENT_OK;
 }
@@ -1245,6 +1295,7 @@ static PushArgs push_args(excent_engine* e, int q) {
     a.hids = e->d_hids; a.hoff = e->d_hoff; a.hedges = e->d_hedges; a.hlist = e->d_hlist;
     a.hubq = e->d_hubq[q]; a.hub_cap = e->hub_cap[q]; a.hub_cnt = e->d_hubcnt + q; a.ctrl = e->d_ctrl;
     a.hub_id = e->d_hub_id; a.hub_k = e->hub_k;
+    a.hubv = e->d_hubv; a.hubv_cnt = e->d_hubv_cnt; a.hubs_first = 0;
     return a;
 }
 
@@ -1372,6 +1423,7 @@ extern "C" int excent_engine_push_stream(excent_engine* e, int s, int c, const u
         k_fill_hot<<<grid, BLOCK, 0, sl.st>>>(hlo, hhi, e->d_hids, e->d_hoff, e->d_idx, e0, dst, e->d_hedges);
         e->launches++;
     }
+    if (to_cache) hub_encode(e, e0, e1, sl.st);   // the cached copy carries the hub-target slots
     const int v0 = e->cv0[c], nv = (c + 1 < e->nc ? e->cv0[c + 1] : e->n) - v0;
     const ull k = cnt[2 * c];
     PushArgs a = push_args(e, 1 + s);
@@ -1483,6 +1535,17 @@ static void enqueue_pass(excent_engine* e, double list_frac, int max_passes, cud
     if (ev) cudaEventRecord(ev[2], st);
     PushArgs a = push_args(e, 0);
     const int gt = e->sms * 8;
+    if (e->hubs_first) {
+        // the high-degree lists first, so their (large) share of the pass's residual reaches
+        // every other vertex before that vertex is taken
+        if (e->L == 1) k_push<1, SRC_HUBS><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
+        else k_push<4, SRC_HUBS><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
+        if (e->L == 1) k_hub<1><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
+        else k_hub<4><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
+        cudaMemsetAsync(a.hub_cnt, 0, sizeof(ull), st);   // the queue is empty again for gather passes
+        e->launches += 2;
+        a.hubs_first = 1;
+    }
     if (e->L == 1) k_push<1, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
     else k_push<4, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
     e->launches++;
@@ -1499,9 +1562,11 @@ static void enqueue_pass(excent_engine* e, double list_frac, int max_passes, cud
         e->launches += 2;
     }
     if (ev) cudaEventRecord(ev[3], st);
-    if (e->L == 1) k_hub<1><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
-    else k_hub<4><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
-    e->launches++;
+    if (!e->hubs_first) {   // with the high-degree lists first, the table push queues no segments
+        if (e->L == 1) k_hub<1><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
+        else k_hub<4><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
+        e->launches++;
+    }
     if (pull_edges > 0) {
         if (e->L == 1) k_pullhub<1><<<e->grid_push, BLOCK, 0, st>>>(e->d_r, e->d_P, a.hubq, a.hub_cnt, a.hub_cap, e->d_ctrl, e->d_hub_id);
         else k_pullhub<4><<<e->grid_push, BLOCK, 0, st>>>(e->d_r, e->d_P, a.hubq, a.hub_cnt, a.hub_cap, e->d_ctrl, e->d_hub_id);
@@ -1589,12 +1654,19 @@ static int solve_impl(excent_engine* e, double list_frac, int max_passes, int us
     EX_CUDA(cudaMemcpyAsync(e->d_cmode, cm.data(), e->nc, cudaMemcpyHostToDevice, e->s_main));
     if (init) EX_TRY(init_state(e));
     else EX_TRY(reset_counters(e));
+    if (e->hubs_first && e->hubv_stale) {
+        EX_CUDA(cudaMemsetAsync(e->d_hubv_cnt, 0, sizeof(ull), e->s_main));
+        k_hub_list<<<e->sms * 8, BLOCK, 0, e->s_main>>>(e->n, e->d_idx, e->d_hubv, e->d_hubv_cnt);
+        e->launches++;
+        EX_CUDA(cudaGetLastError());
+        e->hubv_stale = false;
+    }
     if (use_graph) {
         EX_TRY(build_graph(e, list_frac, max_passes));
         EX_CUDA(cudaGraphLaunch(e->gexec, e->s_main));
         EX_CUDA(cudaStreamSynchronize(e->s_main));
         EX_CUDA(cudaMemcpy(e->h_ctrl, e->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
-        e->launches += (e->pull_frac > 0 && e->d_P ? 7ull : 4ull) * (e->h_ctrl->pass + 1);
+        e->launches += ((e->pull_frac > 0 && e->d_P ? 7ull : 4ull) + (e->hubs_first ? 1ull : 0ull)) * (e->h_ctrl->pass + 1);
     } else {
         for (int p = 0; p <= max_passes; p++) {
             enqueue_pass(e, list_frac, max_passes, 0, 0, e->s_main, e->prof ? e->ev : nullptr);
@@ -1730,25 +1802,35 @@ extern "C" int excent_engine_set_hub_targets(excent_engine* e, int k) {
         std::vector<int> slot_of(e->n, -1);
         for (int i = 0; i < k; i++) slot_of[ids[i]] = i;
         if (!e->d_hub_id) EX_ALLOC(e->d_hub_id, (size_t)kmax * sizeof(int));
-        int* d_slot = nullptr;
-        EX_ALLOC(d_slot, (size_t)e->n * sizeof(int));
-        cudaError_t err = cudaMemcpy(e->d_hub_id, ids.data(), (size_t)k * sizeof(int), cudaMemcpyHostToDevice);
-        if (err == cudaSuccess)
-            err = cudaMemcpy(d_slot, slot_of.data(), (size_t)e->n * sizeof(int), cudaMemcpyHostToDevice);
-        if (err == cudaSuccess) {
-            k_hub_encode<<<e->sms * 8, BLOCK, 0, e->s_main>>>(e->cache_edges, e->d_cache, d_slot);
-            e->launches++;
-            err = cudaStreamSynchronize(e->s_main);
-        }
-        cudaFree(d_slot);
-        EX_CUDA(err);
+        if (!e->d_slot) EX_ALLOC(e->d_slot, (size_t)e->n * sizeof(int));
+        EX_CUDA(cudaMemcpy(e->d_hub_id, ids.data(), (size_t)k * sizeof(int), cudaMemcpyHostToDevice));
+        EX_CUDA(cudaMemcpy(e->d_slot, slot_of.data(), (size_t)e->n * sizeof(int), cudaMemcpyHostToDevice));
         e->hub_k = k;
+        hub_encode(e, 0, e->cache_edges, e->s_main);
+        EX_CUDA(cudaStreamSynchronize(e->s_main));
+        EX_CUDA(cudaGetLastError());
+    } else if (e->d_slot) {
+        cudaFree(e->d_slot);
+        e->d_slot = nullptr;
     }
     const size_t smem = hub_smem(e);
     int occ = 0;
     if (e->L == 1) EX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_push<1, SRC_TABLE>, BLOCK, smem));
     else EX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_push<4, SRC_TABLE>, BLOCK, smem));
     e->grid_push = e->sms * std::max(1, occ);
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_set_hub_order(excent_engine* e, int first) {
+    EX_CHECK_ARG(e, "null engine");
+    EX_CUDA(cudaSetDevice(e->dev));
+    invalidate_graph(e);
+    if (first && !e->d_hubv) {
+        EX_ALLOC(e->d_hubv, (size_t)e->n * sizeof(int));
+        EX_ALLOC(e->d_hubv_cnt, sizeof(ull));
+        e->hubv_stale = true;
+    }
+    e->hubs_first = first != 0;
     return EXCENT_OK;
 }
 

@@ -224,6 +224,13 @@ int excent_engine_read_trace(excent_engine* e, uint16_t* out);
  * the cache turns it off. No reference counterpart. */
 int excent_engine_set_hub_targets(excent_engine* e, int k);
 
+/* High-degree-first order for the device solve: each pass pushes the lists
+ * longer than 256 entries first (and their segments), then every other
+ * pending vertex, so the large share of a pass's residual carried by the
+ * high-degree vertices reaches the others before they are taken. Off by
+ * default. No reference counterpart (the reference pushes chunk by chunk). */
+int excent_engine_set_hub_order(excent_engine* e, int first);
+
 /* Direction-optimised passes for the device solve on a SYMMETRIC graph (every
  * edge stored in both directions): a pass whose pending demand (sum of
  * pending degrees) is at least pull_frac * m runs as a gather. It takes every

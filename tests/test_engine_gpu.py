@@ -381,3 +381,39 @@ def test_hub_targets_match_plain_push(rmat16, measure, k, pull):
     for name in names:
         assert res[(k, name)]["l1_rel"] <= 1.1 * res[(0, name)]["l1_rel"] + 1e-7, (name, res)
         assert res[(k, name)]["top100"] >= 95
+
+
+@pytest.mark.parametrize("measure", ["pr", "all"])
+@pytest.mark.parametrize("use_graph", [True, False])
+@pytest.mark.parametrize("pull", [0.0, 0.3])
+def test_high_degree_first_order(rmat16, measure, use_graph, pull):
+    """Pushing the high-degree lists first in each pass reaches the same fixed
+    point, also with hub targets and with the cache reloaded from host memory
+    (the reload re-encodes the hub-target slots)."""
+    n, idx, adj = rmat16
+    par = O.params(n, idx, adj)
+    kw = dict(alpha=0.9 / par["_lambda"], lam=par["_lambda"], eps_katz=1e-5, eps_ev=1e-5) if measure == "all" else {}
+    names = ["pr", "katz", "ev"] if measure == "all" else ["pr"]
+    assert int((np.diff(idx) > 256).sum()) > 0
+    res = {}
+    for mode in ("plain", "first", "first+targets"):
+        meas = X.measures(measure, **kw)
+        eng = make_engine(n, idx, adj, meas)
+        eng.set_pull(pull)
+        if mode != "plain":
+            eng.set_hub_order(True)
+        if mode == "first+targets":
+            eng.set_hub_targets(512)
+            eng.load_cache(0, len(adj), np.ascontiguousarray(adj, dtype=np.int32))
+        st = eng.solve(use_graph=use_graph)
+        for i, name in enumerate(names):
+            r = eng.read(i, residual=True)
+            assert np.all(np.abs(r) <= np.float32(meas.eps[i]))
+            ref = O.reference_solution(n, idx, adj, name, alpha=kw.get("alpha"))
+            res[(mode, name)] = O.compare(name, ref, eng.read(i))
+        res[(mode, "pushed")] = st.pushed
+        eng.close()
+    print(res)
+    for mode in ("first", "first+targets"):
+        for name in names:
+            assert res[(mode, name)]["l1_rel"] <= 1.1 * res[("plain", name)]["l1_rel"] + 1e-7, (mode, name, res)
