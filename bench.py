@@ -33,6 +33,7 @@ import time
 import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
+LOG_DIR = None   # --log-dir: where CLI runs leave their stdout
 sys.path.insert(0, ROOT)
 
 CONFIGS = {
@@ -78,10 +79,12 @@ def parse():
     ap.add_argument("--ooc-dir", default=None, help="directory for the out-of-core EGR file (default: temp dir)")
     ap.add_argument("--ooc-measures", default="pr", help="comma-separated measures of the out-of-core run")
     ap.add_argument("--ooc-ref", default="on", choices=["on", "off"], help="also run the reference CLI out of core")
-    ap.add_argument("--hub-first", default="off", choices=["on", "off"],
+    ap.add_argument("--log-dir", default=None, help="keep the stdout of every CLI run in this directory")
+    ap.add_argument("--hub-first", default="on", choices=["on", "off"],
                     help="push the high-degree lists first in every pass")
-    ap.add_argument("--hub-targets", type=int, default=0,
-                    help="shared-memory aggregation of the k highest-degree targets (0: off)")
+    ap.add_argument("--hub-targets", type=int, default=-1,
+                    help="shared-memory aggregation of the k highest-degree targets (0: off; -1: 8192 for "
+                         "one measure, 2048 for all)")
     ap.add_argument("--ev-init", default="fp64", choices=["fp64", "reference"],
                     help="eigenvector initial residual from the FP64 lambda1 (default) or from lambda1 rounded to "
                          "float as the reference does")
@@ -188,7 +191,8 @@ def run_ours(a, world, rank, local, dist):
     if v1 is not None and a.ev_project == "on":
         eng.ev_project(v1)
     eng.set_pull(a.pull_frac)
-    eng.set_hub_targets(a.hub_targets)
+    hub_k = a.hub_targets if a.hub_targets >= 0 else min(8192 if nm == 1 else 2048, n)
+    eng.set_hub_targets(hub_k)
     eng.set_hub_order(a.hub_first == "on")
     use_graph = not a.no_graph
     for _ in range(a.warmup):
@@ -278,7 +282,7 @@ def run_ours(a, world, rank, local, dist):
                    "l2_note": "inputs larger than L2 (edge cache %.2f GB)" % (m * 4 / 1e9),
                    "cuda_graph": use_graph, "parallelism": f"{world} independent replicas",
                    "ev_init": a.ev_init, "ev_project": a.ev_project if measure == "all" else None,
-                   "pull_frac": a.pull_frac, "hub_targets": a.hub_targets,
+                   "pull_frac": a.pull_frac, "hub_targets": hub_k,
                    "hub_first": a.hub_first},
         "e2e": {"value": round(e_pushed / te / 1e9, 4), "unit": "GTEPS", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": round(te / a.steps * 1e3, 3),
@@ -329,9 +333,10 @@ def run_ppr(a, world, rank, local, dist):
     vals = [(1 - d) / len(q) for q in qs]
     eps = 1e-4 * (1 - d)
     log(f"graph scale {scale}: n={n} m={m}; {len(qs)} queries on this rank")
-    best, table = X.autotune_batch(n, m, di, da, qs, vals, eps, "ppr", d, device=local)
-    log(f"autotune: per-query ms {table} -> B={best}")
+    best, greedy, table = X.autotune_batch(n, m, di, da, qs, vals, eps, "ppr", d, device=local)
+    log(f"autotune: per-query ms {table} -> B={best} greedy={greedy}")
     b = X.Batch(n, m, di, da, best, "ppr", d, device=local)
+    b.set_greedy(greedy)
     st = torch.cuda.ExternalStream(b.stream())
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     b.seed(qs[:best], vals[:best], eps)   # warm-up (graph build)
@@ -389,7 +394,10 @@ def run_ppr(a, world, rank, local, dist):
         "ms_per_step": round(t_batch * 1e3, 3), "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded R-MAT, generated on the device; query seeds numpy seed 7)",
         "config": {"workload": f"256-query PPR on R-MAT scale {scale} EF {ef} seed {seed}", "n": n, "m": m,
-                   "batch_width": best, "autotune_ms_per_query": table, "passes_per_batch": passes,
+                   "batch_width": best, "greedy": greedy,
+                   "autotune_ms_per_query": {f"B{k[0]}{'_greedy' if k[1] else ''}": round(v, 4)
+                                             for k, v in table.items()},
+                   "passes_per_batch": passes,
                    "pushed_edges": int(tot_e), "queries_per_rank": len(qs)},
         "sequential": {"solves_per_s": round(nq_all / t_seq, 3), "seconds": round(t_seq, 3),
                        "pushed_edges": int(seq_e)},
@@ -493,7 +501,7 @@ def cpu_sample(n, idx, adj, meas, measure, lam, max_edges):
     return pushed, passes, time.perf_counter() - t0
 
 
-def cli_runs(binary, args, reps=2):
+def cli_runs(binary, args, reps=2, log_name=None):
     """Run a CLI `reps` times; keep the run with the shortest pass time."""
     import re
     import subprocess
@@ -508,6 +516,10 @@ def cli_runs(binary, args, reps=2):
         tp = float(re.search(r"time: .* passes ([0-9.]+)s", out).group(1))
         if best is None or tp < best["passes_s"]:
             best = {"passes": passes, "pushed_x_m": xe, "passes_s": tp}
+            keep = out
+    if log_name and LOG_DIR:
+        with open(os.path.join(LOG_DIR, log_name), "w") as f:
+            f.write(keep)
     return best
 
 
@@ -537,7 +549,7 @@ def cli_compare(a, idx, adj, measure, meas, lam, device):
         res = {"args": " ".join(args[1:]), "file_gb": round(os.path.getsize(path) / 1e9, 3)}
         for name, binary, extra in (("reference", ref_bin, []), ("ours", K.CLI_PATH, []),
                                     ("ours_device_loop", K.CLI_PATH, ["--device-loop"])):
-            r = cli_runs(binary, args + extra)
+            r = cli_runs(binary, args + extra, log_name=f"cli_{measure}_{name}.log")
             if "passes_s" in r:
                 r["gteps"] = round(r["pushed_x_m"] * m / r["passes_s"] / 1e9, 3)
             res[name] = r
@@ -666,9 +678,9 @@ def run_ooc(a, world, rank, local, dist):
                 f["gteps"] = round(f["pushed_x_m"] * m / f["passes_s"] / 1e9, 4) if f["passes_s"] else None
                 runs[f"{measure}/{name}"] = f
                 log(f"{measure}/{name}: {f}")
-                with open(os.path.join(ROOT, "gpurun_out", f"ooc_{measure}_{name}.log") if os.path.isdir(
-                        os.path.join(ROOT, "gpurun_out")) else os.devnull, "w") as fo:
-                    fo.write(r.stdout)
+                if LOG_DIR:
+                    with open(os.path.join(LOG_DIR, f"ooc_{measure}_{name}.log"), "w") as fo:
+                        fo.write(r.stdout)
         del ballast
         ours = runs.get(f"{a.ooc_measures.split(',')[0]}/ours", {})
         if "passes_s" not in ours:
@@ -742,7 +754,9 @@ def run_reference(a, world, rank):
 
 
 def main():
+    global LOG_DIR
     a = parse()
+    LOG_DIR = a.log_dir
     world, rank, local, dist = dist_setup(a.gpus)
     if a.impl == "reference":
         res = run_reference(a, world, rank)

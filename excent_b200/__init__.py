@@ -414,14 +414,17 @@ def _pack_queries(seeds, values, eps):
 
 
 def autotune_batch(n, m, d_idx, d_adj, seeds, values, eps, kind="ppr", d_or_alpha=0.85, device=0, max_passes=100000):
-    """Batch width with the lowest time per query on these queries (excent_batch_autotune)."""
+    """Batch width and greedy mode with the lowest time per query on these queries
+    (excent_batch_autotune): (B, greedy, {(B, greedy): ms per query})."""
     off, vids, vals, e = _pack_queries(seeds, values, eps)
     best = C.c_int()
-    ms = np.zeros(4, dtype=np.float64)
+    greedy = C.c_int()
+    ms = np.zeros(8, dtype=np.float64)
     call("excent_batch_autotune", int(device), int(n), int(m), _ptr(d_idx), _ptr(d_adj), {"ppr": 0, "katz": 1}[kind],
          float(d_or_alpha), len(seeds), _ptr(off), _ptr(vids), _ptr(vals), _ptr(e), int(max_passes), C.byref(best),
-         _tp(ms, _capi.f64p))
-    return best.value, dict(zip((32, 64, 128, 256), ms.tolist()))
+         C.byref(greedy), _tp(ms, _capi.f64p))
+    table = {(B, g): ms[2 * i + g] for i, B in enumerate((32, 64, 128, 256)) for g in (0, 1)}
+    return best.value, bool(greedy.value), table
 
 
 def shard(count, world, rank):

@@ -78,7 +78,7 @@ PROTOS = [
     ("excent_batch_launches", C.c_int, [vp, u64p]),
     ("excent_batch_set_greedy", C.c_int, [vp, C.c_int]),
     ("excent_batch_autotune", C.c_int, [C.c_int, C.c_int, u64, vp, vp, C.c_int, C.c_double, C.c_int, vp, vp, vp, vp,
-                                        C.c_int, C.POINTER(C.c_int), f64p]),
+                                        C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), f64p]),
     ("excent_engine_stats", C.c_int, [vp, C.POINTER(Stats), C.POINTER(PassLog), C.c_int]),
     ("excent_engine_read", C.c_int, [vp, C.c_int, C.c_int, vp, u64, u64]),
     ("excent_engine_write", C.c_int, [vp, C.c_int, vp, vp]),

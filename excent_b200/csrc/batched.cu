@@ -575,18 +575,20 @@ extern "C" int excent_batch_launches(excent_batch* b, unsigned long long* launch
 extern "C" int excent_batch_autotune(int device, int n, unsigned long long m, const unsigned long long* d_idx,
                                      const int32_t* d_adj, int kind, double d_or_alpha, int nq, const int* lane_off,
                                      const int32_t* vids, const float* vals, const float* eps, int max_passes,
-                                     int* best_B, double* per_query_ms) {
+                                     int* best_B, int* best_greedy, double* per_query_ms) {
     EX_CHECK_ARG(best_B && nq >= 1 && lane_off, "bad argument");
     const int widths[4] = {32, 64, 128, 256};
     double best = 1e300;
     *best_B = 0;
-    for (int i = 0; i < 4; i++) {
+    if (best_greedy) *best_greedy = 1;
+    for (int i = 0; i < 8; i++) {
         if (per_query_ms) per_query_ms[i] = 0;
-        const int B = widths[i];
+        const int B = widths[i >> 1], greedy = i & 1;
         excent_batch* b = nullptr;
         if (excent_batch_create(device, n, m, d_idx, d_adj, B, kind, d_or_alpha, &b) != EXCENT_OK) continue;
+        int rc = excent_batch_set_greedy(b, greedy);
         const int q = std::min(B, nq);
-        int rc = excent_batch_seed(b, q, lane_off, vids, vals, eps);
+        if (rc == EXCENT_OK) rc = excent_batch_seed(b, q, lane_off, vids, vals, eps);
         cudaEvent_t e0, e1;
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
@@ -608,7 +610,7 @@ extern "C" int excent_batch_autotune(int device, int n, unsigned long long m, co
         if (rc != EXCENT_OK) return rc;
         const double pq = ms / q;
         if (per_query_ms) per_query_ms[i] = pq;
-        if (pq < best) { best = pq; *best_B = B; }
+        if (pq < best) { best = pq; *best_B = B; if (best_greedy) *best_greedy = greedy; }
     }
     if (!*best_B) EX_FAIL(EXCENT_ERR_NOMEM, "autotune: no batch width could be allocated");
     return EXCENT_OK;

@@ -810,19 +810,19 @@ __global__ void k_hub_list(int n, const ull* idx, int* out, ull* cnt) {
 }
 
 // Encode / decode the edge cache for hub-target aggregation.
-__global__ void k_hub_encode(ull m, int* adj, const int* slot_of) {
+__global__ void k_hub_encode(ull m, int* adj, const int* slot_of, int n) {
     for (ull e = blockIdx.x * (ull)blockDim.x + threadIdx.x; e < m; e += (ull)gridDim.x * blockDim.x) {
         const int u = adj[e];
-        if (u >= 0) {
+        if (u >= 0 && u < n) {
             const int sl = slot_of[u];
             if (sl >= 0) adj[e] = (int)(0x80000000u | (unsigned)sl);
         }
     }
 }
-__global__ void k_hub_decode(ull m, int* adj, const int* hub_id) {
+__global__ void k_hub_decode(ull m, int* adj, const int* hub_id, int hub_k) {
     for (ull e = blockIdx.x * (ull)blockDim.x + threadIdx.x; e < m; e += (ull)gridDim.x * blockDim.x) {
         const int u = adj[e];
-        if (u < 0) adj[e] = hub_id[u & HUB_MASK];
+        if (u < 0 && (u & HUB_MASK) < hub_k) adj[e] = hub_id[u & HUB_MASK];
     }
 }
 
@@ -895,7 +895,7 @@ struct excent_engine {
     int hub_k = 0;           // slots in use (0: off)
     int* d_hubv = nullptr;   // high-degree-first order: vertices with lists longer than HUB_MIN
     ull* d_hubv_cnt = nullptr;
-    bool hubs_first = false;
+    bool hubs_first = true;
     bool hubv_stale = true;
     double pull_frac = 0;    // pull when the pending demand >= pull_frac * m (0: never)
     bool ev_proj = false;
@@ -1047,7 +1047,7 @@ static int engine_setup(excent_engine* e, int device, int n, ull m, const excent
 // Encode cache entries [e0, e1) for hub-target aggregation (no-op when off).
 static void hub_encode(excent_engine* e, ull e0, ull e1, cudaStream_t st) {
     if (!e->hub_k || !e->d_slot || e1 <= e0) return;
-    k_hub_encode<<<e->sms * 8, BLOCK, 0, st>>>(e1 - e0, e->d_cache + e0, e->d_slot);
+    k_hub_encode<<<e->sms * 8, BLOCK, 0, st>>>(e1 - e0, e->d_cache + e0, e->d_slot, e->n);
     e->launches++;
 }
 
@@ -1654,6 +1654,11 @@ static int solve_impl(excent_engine* e, double list_frac, int max_passes, int us
     EX_CUDA(cudaMemcpyAsync(e->d_cmode, cm.data(), e->nc, cudaMemcpyHostToDevice, e->s_main));
     if (init) EX_TRY(init_state(e));
     else EX_TRY(reset_counters(e));
+    if (e->hubs_first && !e->d_hubv) {
+        EX_ALLOC(e->d_hubv, (size_t)e->n * sizeof(int));
+        EX_ALLOC(e->d_hubv_cnt, sizeof(ull));
+        e->hubv_stale = true;
+    }
     if (e->hubs_first && e->hubv_stale) {
         EX_CUDA(cudaMemsetAsync(e->d_hubv_cnt, 0, sizeof(ull), e->s_main));
         k_hub_list<<<e->sms * 8, BLOCK, 0, e->s_main>>>(e->n, e->d_idx, e->d_hubv, e->d_hubv_cnt);
@@ -1781,14 +1786,19 @@ extern "C" int excent_engine_set_hub_targets(excent_engine* e, int k) {
     EX_CUDA(cudaSetDevice(e->dev));
     EX_CUDA(cudaDeviceSynchronize());
     invalidate_graph(e);
-    if (e->hub_k && e->d_cache && e->cache_edges) {   // back to plain ids first
-        k_hub_decode<<<e->sms * 8, BLOCK, 0, e->s_main>>>(e->cache_edges, e->d_cache, e->d_hub_id);
-        e->launches++;
+    if (e->hub_k && e->d_cache && e->cache_edges) {   // back to plain ids first (loaded chunks only)
+        for (int c = 0; c < e->nc; c++) {
+            if (!e->loaded[c] || e->ce[c + 1] > e->cache_edges || e->ce[c + 1] == e->ce[c]) continue;
+            k_hub_decode<<<e->sms * 8, BLOCK, 0, e->s_main>>>(e->ce[c + 1] - e->ce[c], e->d_cache + e->ce[c],
+                                                               e->d_hub_id, e->hub_k);
+            e->launches++;
+        }
         EX_CUDA(cudaStreamSynchronize(e->s_main));
+        EX_CUDA(cudaGetLastError());
     }
     e->hub_k = 0;
     if (k > 0) {
-        EX_CHECK_ARG(e->d_cache && e->cache_edges, "load the edge cache before choosing hub targets");
+        EX_CHECK_ARG(e->d_cache && e->cache_edges, "reserve the edge cache before choosing hub targets");
         std::vector<ull> idx((size_t)e->n + 1);
         EX_CUDA(cudaMemcpy(idx.data(), e->d_idx, idx.size() * sizeof(ull), cudaMemcpyDeviceToHost));
         std::vector<int> ids(e->n);
@@ -1806,7 +1816,8 @@ extern "C" int excent_engine_set_hub_targets(excent_engine* e, int k) {
         EX_CUDA(cudaMemcpy(e->d_hub_id, ids.data(), (size_t)k * sizeof(int), cudaMemcpyHostToDevice));
         EX_CUDA(cudaMemcpy(e->d_slot, slot_of.data(), (size_t)e->n * sizeof(int), cudaMemcpyHostToDevice));
         e->hub_k = k;
-        hub_encode(e, 0, e->cache_edges, e->s_main);
+        for (int c = 0; c < e->nc; c++)   // chunks loaded so far; later loads encode themselves
+            if (e->loaded[c] && e->ce[c + 1] <= e->cache_edges) hub_encode(e, e->ce[c], e->ce[c + 1], e->s_main);
         EX_CUDA(cudaStreamSynchronize(e->s_main));
         EX_CUDA(cudaGetLastError());
     } else if (e->d_slot) {
@@ -1825,11 +1836,6 @@ extern "C" int excent_engine_set_hub_order(excent_engine* e, int first) {
     EX_CHECK_ARG(e, "null engine");
     EX_CUDA(cudaSetDevice(e->dev));
     invalidate_graph(e);
-    if (first && !e->d_hubv) {
-        EX_ALLOC(e->d_hubv, (size_t)e->n * sizeof(int));
-        EX_ALLOC(e->d_hubv_cnt, sizeof(ull));
-        e->hubv_stale = true;
-    }
     e->hubs_first = first != 0;
     return EXCENT_OK;
 }

@@ -42,6 +42,8 @@ struct Options {
     double budget_gb = 0;      // cap on the free device memory used for sizing (0: none)
     bool device_loop = false;  // fully cached graphs: load at setup, run the on-device pass loop
     bool ev_init_fp64 = false; // eigenvector initial residual from the FP64 lambda1
+    int hub_targets = -1;      // shared-memory aggregation of the top-degree targets (-1: auto)
+    bool hub_first = true;     // device loop: push the high-degree lists first in every pass
 };
 
 static const char* USAGE =
@@ -98,6 +100,20 @@ static int parse_options(int argc, char** argv, Options& o) {
         else if (a == "--device") { if ((ok = next(v))) o.device = atoi(v); }
         else if (a == "--gpu-budget-gb") { if ((ok = next(v))) o.budget_gb = atof(v); }
         else if (a == "--device-loop") o.device_loop = true;
+        else if (a == "--hub-targets") {
+            if ((ok = next(v))) {
+                if (!strcmp(v, "auto")) o.hub_targets = -1;
+                else if (!strcmp(v, "off")) o.hub_targets = 0;
+                else o.hub_targets = atoi(v);
+                if (o.hub_targets < -1) { fprintf(stderr, "--hub-targets must be auto, off or a count\n"); return 1; }
+            }
+        }
+        else if (a == "--hub-first") {
+            if ((ok = next(v))) {
+                if (strcmp(v, "on") && strcmp(v, "off")) { fprintf(stderr, "--hub-first must be on or off\n"); return 1; }
+                o.hub_first = !strcmp(v, "on");
+            }
+        }
         else if (a == "--ev-init") {
             if ((ok = next(v))) {
                 if (strcmp(v, "fp64") && strcmp(v, "reference")) { fprintf(stderr, "--ev-init must be fp64 or reference\n"); return 1; }
@@ -216,7 +232,12 @@ static int run(const Options& o) {
             n_resident--;   // the allocation failed: keep fewer chunks
         }
         for (int c = 0; c < n_resident; c++) { resident[c] = 1; resident_edges += chunks[c].edges(); }
+        if (n_resident > 0) {   // shared-memory sums for the top-degree targets of cached pushes
+            const int k = o.hub_targets < 0 ? std::min(M.nm == 1 ? 8192 : 2048, n) : o.hub_targets;
+            if (k > 0) RT_CK(excent_engine_set_hub_targets(e, k));
+        }
     }
+    RT_CK(excent_engine_set_hub_order(e, o.hub_first ? 1 : 0));
     int nh = 0;
     ull hot_edges = 0, hot_deg_min = 0;
     bool hot_mode = hot_mode_req;

@@ -227,7 +227,7 @@ int excent_engine_set_hub_targets(excent_engine* e, int k);
 /* High-degree-first order for the device solve: each pass pushes the lists
  * longer than 256 entries first (and their segments), then every other
  * pending vertex, so the large share of a pass's residual carried by the
- * high-degree vertices reaches the others before they are taken. Off by
+ * high-degree vertices reaches the others before they are taken. On by
  * default. No reference counterpart (the reference pushes chunk by chunk). */
 int excent_engine_set_hub_order(excent_engine* e, int first);
 
@@ -369,11 +369,14 @@ int excent_batch_stream(excent_batch* b, void** stream);
  * |r| <= eps. */
 int excent_batch_set_greedy(excent_batch* b, int greedy);
 /* Autotuner: time one batch of min(B, nq) of the given queries (seeded as
- * in excent_batch_seed) at each width B in {32, 64, 128, 256} and return the
- * width with the lowest time per query; per_query_ms[4] gets the times. */
+ * in excent_batch_seed) at each width B in {32, 64, 128, 256}, with the
+ * greedy whole-row push off and on, and return the pair with the lowest time
+ * per query (best_greedy may be NULL); per_query_ms[8] gets the times, entry
+ * 2*i + greedy for width i. */
 int excent_batch_autotune(int device, int n, unsigned long long m, const unsigned long long* d_idx, const int32_t* d_adj,
                           int kind, double d_or_alpha, int nq, const int* lane_off, const int32_t* vids,
-                          const float* vals, const float* eps, int max_passes, int* best_B, double* per_query_ms);
+                          const float* vals, const float* eps, int max_passes, int* best_B, int* best_greedy,
+                          double* per_query_ms);
 int excent_batch_launches(excent_batch* b, unsigned long long* launches);
 
 /* ------------------------------------------------------------ adjoint (VJP) */

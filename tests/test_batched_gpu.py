@@ -104,3 +104,16 @@ def test_batched_katz_beta_vector(dgraph):
         x = b.read(q)
         assert np.abs(x - ref).max() <= 1e-4 * max(1.0, np.abs(ref).max())
     b.close()
+
+
+def test_autotuner_picks_a_width_and_mode(rmat16):
+    n, idx, adj = rmat16
+    d_idx = torch.from_numpy(idx.astype(np.int64)).cuda()
+    d_adj = torch.from_numpy(adj).cuda()
+    rng = np.random.default_rng(3)
+    seeds = [np.sort(rng.choice(n, int(k), replace=False)).astype(np.int32) for k in rng.integers(1, 64, 40)]
+    vals = [0.15 / len(q) for q in seeds]
+    B, greedy, table = X.autotune_batch(n, len(adj), d_idx.data_ptr(), d_adj.data_ptr(), seeds, vals, 1e-4 * 0.15)
+    assert B in (32, 64, 128, 256) and greedy in (False, True)
+    assert len(table) == 8 and all(v > 0 for v in table.values())
+    assert table[(B, int(greedy))] == min(table.values())

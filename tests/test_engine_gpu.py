@@ -400,8 +400,7 @@ def test_high_degree_first_order(rmat16, measure, use_graph, pull):
         meas = X.measures(measure, **kw)
         eng = make_engine(n, idx, adj, meas)
         eng.set_pull(pull)
-        if mode != "plain":
-            eng.set_hub_order(True)
+        eng.set_hub_order(mode != "plain")
         if mode == "first+targets":
             eng.set_hub_targets(512)
             eng.load_cache(0, len(adj), np.ascontiguousarray(adj, dtype=np.int32))
