@@ -384,6 +384,13 @@ def run_ppr(a, world, rank, local, dist):
     t_seq = ev0.elapsed_time(ev1) / 1e3
     log(f"sequential: {len(qs)} queries in {t_seq:.3f}s")
     diff = [float(np.abs(xb[j].astype(np.float64) - xs[j]).sum()) for j in range(len(xb))]
+    # the FP64 oracle of those queries on the device (Jacobi to 1e-10), L1 error relative to its mass
+    l1b, l1s = [], []
+    for j in range(len(xb)):
+        ref, _ = X.ppr_fp64(n, di, da, qs[j], vals[j], d=d, tol=1e-10, device=local)
+        mass = float(np.abs(ref).sum())
+        l1b.append(float(np.abs(xb[j] - ref).sum()) / mass)
+        l1s.append(float(np.abs(xs[j] - ref).sum()) / mass)
     if dist:
         tt = torch.tensor([t_batch, t_seq], device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -403,6 +410,7 @@ def run_ppr(a, world, rank, local, dist):
                        "pushed_edges": int(seq_e)},
         "speedup_vs_sequential": round(t_seq / t_batch, 2),
         "l1_batched_minus_sequential": diff,
+        "l1_rel_vs_fp64_oracle": {"batched": l1b, "sequential": l1s, "queries": "the first 4"},
     }
     b.close()
     eng.close()

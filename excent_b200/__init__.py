@@ -235,6 +235,18 @@ class Engine:
         return dict(zip(("snapshot", "plan", "push", "hub"), ms.tolist())), p.value
 
 
+def ppr_fp64(n, d_idx, d_adj, seeds, values, d=0.85, tol=1e-10, maxit=2000, device=0):
+    """FP64 personalized PageRank of one seed set on a device graph (excent_ppr_fp64); values is a
+    scalar (the same residual at every seed) or one value per seed."""
+    seeds = np.ascontiguousarray(seeds, dtype=np.int32)
+    vals = np.ascontiguousarray(np.broadcast_to(np.float32(values), seeds.shape), dtype=np.float32)
+    x = np.empty(n, dtype=np.float64)
+    it = C.c_int()
+    call("excent_ppr_fp64", int(device), int(n), _ptr(d_idx), _ptr(d_adj), float(d), len(seeds), _ptr(seeds),
+         _ptr(vals), float(tol), int(maxit), _tp(x, _capi.f64p), C.byref(it))
+    return x, it.value
+
+
 def write_egr(path, idx, adj, wide=True):
     """Write a CSR graph as an EGR file (README.md:136-146): int32 n, then int32 -1 and int64 m
     with uint64 offsets (wide), or int32 m with uint32 offsets (narrow); then int32 lists."""

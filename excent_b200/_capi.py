@@ -126,6 +126,8 @@ PROTOS = [
     ("excent_cli_main", C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
     ("excent_rmat_generate", C.c_int, [C.c_int, C.c_int, C.c_int, u64, C.c_double, C.c_double, C.c_double,
                                        C.c_int, C.c_int, C.POINTER(vp)]),
+    ("excent_ppr_fp64", C.c_int, [C.c_int, C.c_int, vp, vp, C.c_double, C.c_int, vp, vp, C.c_double, C.c_int, vp,
+                                  C.POINTER(C.c_int)]),
     ("excent_rmat_write_egr", C.c_int, [C.c_int, C.c_int, C.c_int, u64, C.c_double, C.c_double, C.c_double, u64,
                                         C.c_char_p, u64p, C.POINTER(C.c_int)]),
     ("excent_dgraph_info", C.c_int, [vp, C.POINTER(C.c_int), u64p]),

@@ -17,10 +17,11 @@
 
 namespace excent {
 
-// y[v] = c + s * sum_{u in N(v)} x[u] (/ L(u) if divdeg); one warp per vertex.
+// y[v] = c + s * sum_{u in N(v)} x[u] (/ L(u) if divdeg), c[v] from cv if given;
+// one warp per vertex.
 // If mx is given: mx[0] = max |y - x|, mx[1] = max |y| (as ordered bit patterns).
 __global__ void k_pull64(int n, const ull* idx, const int* adj, const double* x, double* y, double c, double s,
-                         int divdeg, ull* mx) {
+                         int divdeg, ull* mx, const double* cv = nullptr) {
     const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= n) return;
@@ -31,7 +32,7 @@ __global__ void k_pull64(int n, const ull* idx, const int* adj, const double* x,
     }
     acc = warp_sum(acc);
     if (lane == 0) {
-        const double nv = c + s * acc;
+        const double nv = (cv ? cv[w] : c) + s * acc;
         y[w] = nv;
         if (mx) {
             atomicMax(&mx[0], (ull)__double_as_longlong(fabs(nv - x[w])));
@@ -197,4 +198,62 @@ extern "C" int excent_reference_fp64(int device, int n, const unsigned long long
     }
     if (iterations) *iterations = it;
     return EXCENT_OK;
+}
+
+__global__ void k_scatter64(int k, const int* vids, const float* vals, double* t) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) t[vids[i]] += (double)vals[i];
+}
+
+extern "C" int excent_ppr_fp64(int device, int n, const unsigned long long* d_idx, const int32_t* d_adj, double d,
+                               int k, const int32_t* vids, const float* vals, double tol, int maxit, double* x_out,
+                               int* iterations) {
+    EX_CHECK_ARG(n >= 1 && d_idx && d_adj && x_out && k >= 0 && (k == 0 || (vids && vals)), "bad argument");
+    for (int i = 0; i < k; i++) EX_CHECK_ARG(vids[i] >= 0 && vids[i] < n, "seed vertex %d out of range", vids[i]);
+    EX_CUDA(cudaSetDevice(device));
+    int sms = 0;
+    EX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const int G = sms * 8;
+    const unsigned wb = (unsigned)(((long long)n * 32 + 255) / 256);
+    Bufs B;
+    double* t = nullptr;
+    int* dv = nullptr;
+    float* dval = nullptr;
+    for (auto& p : B.v) if (cudaMalloc(&p, (size_t)n * sizeof(double)) != cudaSuccess) { cudaGetLastError(); EX_FAIL(EXCENT_ERR_NOMEM, "ppr reference: vectors do not fit"); }
+    EX_CUDA(cudaMalloc(&B.red, 2 * sizeof(double)));
+    EX_CUDA(cudaMalloc(&B.mx, 2 * sizeof(ull)));
+    int rc = EXCENT_OK;
+    int it = 0;
+    do {
+        if (cudaMalloc(&t, (size_t)n * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&dv, std::max(k, 1) * sizeof(int)) != cudaSuccess ||
+            cudaMalloc(&dval, std::max(k, 1) * sizeof(float)) != cudaSuccess) {
+            cudaGetLastError(); set_error("ppr reference: teleport vector does not fit"); rc = EXCENT_ERR_NOMEM; break;
+        }
+        cudaMemset(t, 0, (size_t)n * sizeof(double));
+        if (k) {
+            cudaMemcpy(dv, vids, (size_t)k * sizeof(int), cudaMemcpyHostToDevice);
+            cudaMemcpy(dval, vals, (size_t)k * sizeof(float), cudaMemcpyHostToDevice);
+            k_scatter64<<<std::min(1024, (k + 255) / 256), 256>>>(k, dv, dval, t);
+        }
+        cudaMemcpy(B.v[0], t, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice);
+        double rel = 1;
+        for (; it < maxit && rel > tol; it++) {
+            cudaMemset(B.mx, 0, 2 * sizeof(ull));
+            k_pull64<<<wb, 256>>>(n, d_idx, d_adj, B.v[0], B.v[1], 0.0, d, 1, B.mx, t);
+            ull h[2];
+            if (cudaMemcpy(h, B.mx, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess) break;
+            double dd, mm;
+            memcpy(&dd, &h[0], 8);
+            memcpy(&mm, &h[1], 8);
+            rel = mm > 0 ? dd / mm : 0.0;
+            std::swap(B.v[0], B.v[1]);
+        }
+        const cudaError_t err = cudaMemcpy(x_out, B.v[0], (size_t)n * sizeof(double), cudaMemcpyDeviceToHost);
+        if (err != cudaSuccess) { set_error("ppr reference: %s", cudaGetErrorString(err)); rc = EXCENT_ERR_CUDA; }
+    } while (0);
+    if (t) cudaFree(t);
+    if (dv) cudaFree(dv);
+    if (dval) cudaFree(dval);
+    if (iterations) *iterations = it;
+    return rc;
 }

@@ -450,6 +450,14 @@ int excent_params_fp64_noalloc(int device, int n, const unsigned long long* d_id
 int excent_reference_fp64(int device, int n, const unsigned long long* d_idx, const int32_t* d_adj, int kind,
                           double alpha, double beta, double tol, int maxit, double* x_out, int* iterations);
 
+/* FP64 personalized PageRank on the device: Jacobi on x = t + d sum x_u / L(u)
+ * with t[v] = the sum of vals over the k seeds at v (the seeded solve's
+ * initial residual), from x = t until max|dx| / max|x| <= tol or maxit. The
+ * oracle of batched and seeded solves on graphs too large for the CPU one.
+ * x_out: n doubles on the host. */
+int excent_ppr_fp64(int device, int n, const unsigned long long* d_idx, const int32_t* d_adj, double d, int k,
+                    const int32_t* vids, const float* vals, double tol, int maxit, double* x_out, int* iterations);
+
 /* ------------------------------------------------------------ R-MAT graphs */
 
 /* A graph held in device memory (CSR offsets, lists, optional weights). */

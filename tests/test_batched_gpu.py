@@ -117,3 +117,17 @@ def test_autotuner_picks_a_width_and_mode(rmat16):
     assert B in (32, 64, 128, 256) and greedy in (False, True)
     assert len(table) == 8 and all(v > 0 for v in table.values())
     assert table[(B, int(greedy))] == min(table.values())
+
+
+def test_device_fp64_ppr_matches_cpu_oracle(dgraph):
+    g, idx, adj = dgraph
+    n = g.n
+    d = 0.85
+    di, da, _ = g.device_ptrs()
+    for q in queries(n, 3, 11, max_size=200):
+        x, it = X.ppr_fp64(n, di, da, q, (1 - d) / len(q), d=d, tol=1e-13)
+        t = np.zeros(n)
+        t[q] = 1.0 / len(q)
+        ref = O.ppr(n, idx, adj, t, kind=0, d=d)
+        assert it > 10
+        assert np.abs(x - ref).max() <= 1e-10 * max(ref.max(), 1e-30) + 1e-14
