@@ -347,11 +347,14 @@ def run_ppr(a, world, rank, local, dist):
     ev0.record(st)
     tot_e = 0
     passes = []
+    counters = {"pushed_vertices": 0, "lane_updates": 0, "rows_checked": 0}
     for i in range(0, len(qs), best):
         b.seed(qs[i:i + best], vals[i:i + best], eps)
         s = b.solve()
         tot_e += s["pushed_edges"]
         passes.append(s["passes"])
+        for k in counters:
+            counters[k] += s[k]
     ev1.record(st)
     torch.cuda.synchronize()
     t_batch = ev0.elapsed_time(ev1) / 1e3
@@ -405,7 +408,7 @@ def run_ppr(a, world, rank, local, dist):
                    "autotune_ms_per_query": {f"B{k[0]}{'_greedy' if k[1] else ''}": round(v, 4)
                                              for k, v in table.items()},
                    "passes_per_batch": passes,
-                   "pushed_edges": int(tot_e), "queries_per_rank": len(qs)},
+                   "pushed_edges": int(tot_e), "queries_per_rank": len(qs), **counters},
         "sequential": {"solves_per_s": round(nq_all / t_seq, 3), "seconds": round(t_seq, 3),
                        "pushed_edges": int(seq_e)},
         "speedup_vs_sequential": round(t_seq / t_batch, 2),

@@ -370,9 +370,10 @@ class Batch:
 
     def stats(self):
         p = C.c_int()
-        v, e, u = C.c_uint64(), C.c_uint64(), C.c_uint64()
-        call("excent_batch_stats", self.h, C.byref(p), C.byref(v), C.byref(e), C.byref(u))
-        return {"passes": p.value, "pushed_vertices": v.value, "pushed_edges": e.value, "lane_updates": u.value}
+        v, e, u, c = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint64()
+        call("excent_batch_stats", self.h, C.byref(p), C.byref(v), C.byref(e), C.byref(u), C.byref(c))
+        return {"passes": p.value, "pushed_vertices": v.value, "pushed_edges": e.value, "lane_updates": u.value,
+                "rows_checked": c.value}
 
     def read(self, lane, residual=False, out=None):
         if out is None:

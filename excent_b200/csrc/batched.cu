@@ -45,6 +45,7 @@ struct BCtrl {
     ull pushed_v[2];          // vertices pushed, by pass parity
     ull hub_rows[2], hub_segs[2];
     ull total_v, total_e, total_lane_e;  // totals over the solve
+    ull rows_checked;                    // touched rows examined, over the solve
     int err;
     int done;
 };
@@ -113,7 +114,7 @@ __global__ void __launch_bounds__(BB) k_bpass(BArgs a) {
     const int par = a.ctrl->pass & 1;
     uint32_t* cur = a.touched[par];
     uint32_t* nxt = a.touched[par ^ 1];
-    ull pushed_v = 0, pushed_e = 0, upd = 0;
+    ull pushed_v = 0, pushed_e = 0, upd = 0, checked = 0;
     float4 eps[NV];
 #pragma unroll
     for (int k = 0; k < NV; k++) eps[k] = a.eps[j0 + LPR * k];
@@ -121,7 +122,7 @@ __global__ void __launch_bounds__(BB) k_bpass(BArgs a) {
         uint32_t bits = cur[w];
         if (!bits) continue;
         __syncwarp();
-        if (lane == 0) cur[w] = 0;
+        if (lane == 0) { cur[w] = 0; checked += __popc(bits); }
         while (bits) {
             const int b = __ffs(bits) - 1;
             bits &= bits - 1;
@@ -210,18 +211,20 @@ __global__ void __launch_bounds__(BB) k_bpass(BArgs a) {
             upd += scatter_rows<LPR, NV>(a, nxt, nb, deg, p, act, lane);
         }
     }
-    __shared__ ull s_v[BB / 32], s_e[BB / 32], s_u[BB / 32];
+    __shared__ ull s_v[BB / 32], s_e[BB / 32], s_u[BB / 32], s_c[BB / 32];
     pushed_v = warp_sum(pushed_v);
     pushed_e = warp_sum(pushed_e);
     upd = warp_sum(upd);
-    if (lane == 0) { s_v[wib] = pushed_v; s_e[wib] = pushed_e; s_u[wib] = upd; }
+    checked = warp_sum(checked);
+    if (lane == 0) { s_v[wib] = pushed_v; s_e[wib] = pushed_e; s_u[wib] = upd; s_c[wib] = checked; }
     __syncthreads();
     if (threadIdx.x == 0) {
-        ull tv = 0, te = 0, tu = 0;
-        for (int i = 0; i < BB / 32; i++) { tv += s_v[i]; te += s_e[i]; tu += s_u[i]; }
+        ull tv = 0, te = 0, tu = 0, tc = 0;
+        for (int i = 0; i < BB / 32; i++) { tv += s_v[i]; te += s_e[i]; tu += s_u[i]; tc += s_c[i]; }
         if (tv) atomicAdd(&a.ctrl->pushed_v[par], tv);
         if (te) atomicAdd(&a.ctrl->total_e, te);
         if (tu) atomicAdd(&a.ctrl->total_lane_e, tu);
+        if (tc) atomicAdd(&a.ctrl->rows_checked, tc);
     }
 }
 
@@ -523,7 +526,8 @@ extern "C" int excent_batch_solve(excent_batch* b, int max_passes, int use_graph
 }
 
 extern "C" int excent_batch_stats(excent_batch* b, int* passes, unsigned long long* pushed_vertices,
-                                  unsigned long long* pushed_edges, unsigned long long* lane_updates) {
+                                  unsigned long long* pushed_edges, unsigned long long* lane_updates,
+                                  unsigned long long* rows_checked) {
     EX_CHECK_ARG(b, "null batch");
     EX_CUDA(cudaSetDevice(b->dev));
     BCtrl c;
@@ -533,6 +537,7 @@ extern "C" int excent_batch_stats(excent_batch* b, int* passes, unsigned long lo
     if (pushed_vertices) *pushed_vertices = c.total_v;
     if (pushed_edges) *pushed_edges = c.total_e;
     if (lane_updates) *lane_updates = c.total_lane_e;
+    if (rows_checked) *rows_checked = c.rows_checked;
     return EXCENT_OK;
 }
 
