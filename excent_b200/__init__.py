@@ -210,6 +210,23 @@ class Engine:
         """Device solve: push the lists longer than 256 entries first in every pass."""
         call("excent_engine_set_hub_order", self.h, int(bool(first)))
 
+    def host_cache(self):
+        """Pinned host memory for the entries past the edge cache (excent_engine_host_cache):
+        returns (numpy int32 view to fill, first edge index)."""
+        p = C.c_void_p()
+        first = C.c_uint64()
+        call("excent_engine_host_cache", self.h, C.byref(p), C.byref(first))
+        cnt = self.m - first.value
+        if not cnt:
+            return np.empty(0, dtype=np.int32), first.value
+        buf = (C.c_int32 * cnt).from_address(p.value)
+        return np.ctypeslib.as_array(buf), first.value
+
+    def host_pushed(self):
+        v = C.c_uint64()
+        call("excent_engine_host_pushed", self.h, C.byref(v))
+        return v.value
+
     def set_pull(self, frac):
         """Gather passes when the pending demand >= frac * m (symmetric graphs only; 0 = never)."""
         call("excent_engine_set_pull", self.h, float(frac))

@@ -146,12 +146,17 @@ __global__ void __launch_bounds__(BB) k_bpass(BArgs a) {
             for (int k = 0; k < NV; k++) {
                 d[k] = make_float4(0.f, 0.f, 0.f, 0.f);
                 if (lane < LPR && row_pend) {
-                    const float4 th = a.greedy ? floor0 : eps[k];
-                    float* rp = reinterpret_cast<float*>(rrow + j0 + LPR * k);
-                    d[k].x = take_lane(rp, rv[k].x, th.x);
-                    d[k].y = take_lane(rp + 1, rv[k].y, th.y);
-                    d[k].z = take_lane(rp + 2, rv[k].z, th.z);
-                    d[k].w = take_lane(rp + 3, rv[k].w, th.w);
+                    if (a.greedy) {
+                        // the whole 16-byte group in one exchange when any of its lanes is nonzero
+                        if (nonzero(rv[k])) d[k] = atomicExch(rrow + j0 + LPR * k, floor0);
+                    } else {
+                        const float4 th = eps[k];
+                        float* rp = reinterpret_cast<float*>(rrow + j0 + LPR * k);
+                        d[k].x = take_lane(rp, rv[k].x, th.x);
+                        d[k].y = take_lane(rp + 1, rv[k].y, th.y);
+                        d[k].z = take_lane(rp + 2, rv[k].z, th.z);
+                        d[k].w = take_lane(rp + 3, rv[k].w, th.w);
+                    }
                     if (nonzero(d[k])) {
                         float4* xp = a.X + (size_t)v * a.V + j0 + LPR * k;
                         float4 xv = *xp;

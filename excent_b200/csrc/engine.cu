@@ -51,6 +51,7 @@ struct Ctrl {
     unsigned pad2;
     double ev_dot;     // FP64 (r_ev . v1) accumulated by the snapshot
     double ev_corr;    // component removed from r_ev by the next snapshot
+    ull host_pushed;   // entries pushed from lists read in place in host memory
 };
 
 struct PassRec {
@@ -117,7 +118,15 @@ struct PushArgs {
     const int* hubv;
     const ull* hubv_cnt;
     int hubs_first;
+    // lists past the device cache read in place from pinned host memory (zero copy)
+    const int* hcache;   // entries [cache_edges, m), device-mapped
+    ull cache_edges;
 };
+
+// Where list b (an edge offset) lives: the HBM cache prefix, or host memory past it.
+__device__ __forceinline__ const int* list_at(const PushArgs& a, ull b) {
+    return b < a.cache_edges ? a.cache + b : a.hcache + (b - a.cache_edges);
+}
 
 // Shared accumulators of the hub targets: zero at kernel start ...
 template <typename T>
@@ -391,7 +400,7 @@ __device__ __forceinline__ bool get_item(const PushArgs& a, long long t, int& v,
         }
         const ull b = a.idx[v];
         deg = a.idx[v + 1] - b;
-        nb = a.cache + b;
+        nb = list_at(a, b);
         return true;
     } else if constexpr (SRC == SRC_CHUNK) {
         if (t >= (long long)a.ccount) return false;
@@ -416,7 +425,7 @@ __device__ __forceinline__ bool get_item(const PushArgs& a, long long t, int& v,
         v = a.hubv[t];
         const ull b = a.idx[v];
         deg = a.idx[v + 1] - b;
-        nb = a.cache + b;
+        nb = list_at(a, b);
         return true;
     } else {
         if (t >= (long long)a.ctrl->hcount) return false;
@@ -460,7 +469,7 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
     const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     const long long total = item_total<SRC>(a);
-    ull pushed = 0;
+    ull pushed = 0, hpushed = 0;
     for (long long tile = gw; tile * 32 < total; tile += nwarps) {
         int v = 0;
         const int* nb = nullptr;
@@ -472,7 +481,10 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
             p = take(x, r, v, deg, a.M);
             act = nonzero(p) && deg > 0;
         }
-        if (act) pushed += deg;
+        if (act) {
+            pushed += deg;
+            if ((SRC == SRC_TABLE || SRC == SRC_HUBS) && a.hcache && a.idx[v] >= a.cache_edges) hpushed += deg;
+        }
         const bool large = act && deg > HUB_MIN;
         if (large) {
             const unsigned nseg = (unsigned)((deg + HUB_SEG - 1) / HUB_SEG);
@@ -528,6 +540,10 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
     }
     pushed = warp_sum(pushed);
     if (lane == 0) s_pushed[wib] = pushed;
+    if (a.hcache) {   // rare path (zero-copy host lists): one atomic per warp
+        hpushed = warp_sum(hpushed);
+        if (lane == 0 && hpushed) atomicAdd(&a.ctrl->host_pushed, hpushed);
+    }
     hacc_flush(hacc, r, a.hub_id, a.hub_k);
     if (threadIdx.x == 0) {
         ull t = 0;
@@ -893,6 +909,8 @@ struct excent_engine {
     int* d_hub_id = nullptr; // hub-target aggregation: vertex of each slot
     int* d_slot = nullptr;   // slot of each vertex (-1: none), kept to encode later cache loads
     int hub_k = 0;           // slots in use (0: off)
+    int* h_hcache = nullptr; // pinned, mapped host copy of the entries past the device cache
+    ull hcache_edges = 0;
     int* d_hubv = nullptr;   // high-degree-first order: vertices with lists longer than HUB_MIN
     ull* d_hubv_cnt = nullptr;
     bool hubs_first = true;
@@ -965,6 +983,7 @@ static int free_engine(excent_engine* e) {
         if (s.done) cudaEventDestroy(s.done);
     }
     for (cudaEvent_t ev : e->ev) if (ev) cudaEventDestroy(ev);
+    if (e->h_hcache) cudaFreeHost(e->h_hcache);
     if (e->s_main) cudaStreamDestroy(e->s_main);
     delete e;
     return EXCENT_OK;
@@ -1138,6 +1157,7 @@ extern "C" int excent_engine_reserve_cache(excent_engine* e, unsigned long long 
     if (e->d_cache) { cudaFree(e->d_cache); e->d_cache = nullptr; e->cache_edges = 0; }
     e->hub_k = 0;   // a fresh cache holds plain ids
     if (e->d_slot) { cudaFree(e->d_slot); e->d_slot = nullptr; }
+    if (e->h_hcache) { cudaFreeHost(e->h_hcache); e->h_hcache = nullptr; e->hcache_edges = 0; }
     if (edges == 0) return EXCENT_OK;
     if (cudaMalloc((void**)&e->d_cache, edges * sizeof(int)) != cudaSuccess) {
         cudaGetLastError();
@@ -1296,6 +1316,8 @@ static PushArgs push_args(excent_engine* e, int q) {
     a.hubq = e->d_hubq[q]; a.hub_cap = e->hub_cap[q]; a.hub_cnt = e->d_hubcnt + q; a.ctrl = e->d_ctrl;
     a.hub_id = e->d_hub_id; a.hub_k = e->hub_k;
     a.hubv = e->d_hubv; a.hubv_cnt = e->d_hubv_cnt; a.hubs_first = 0;
+    a.hcache = nullptr; a.cache_edges = e->cache_edges;
+    if (e->h_hcache) cudaHostGetDevicePointer((void**)&a.hcache, e->h_hcache, 0);
     return a;
 }
 
@@ -1527,7 +1549,7 @@ static void enqueue_pass(excent_engine* e, double list_frac, int max_passes, cud
     if (ev) cudaEventRecord(ev[0], st);
     launch_snapshot(e, false, st);
     if (ev) cudaEventRecord(ev[1], st);
-    const double pull_edges = e->pull_frac > 0 && e->d_P ? e->pull_frac * (double)e->m : 0.0;
+    const double pull_edges = e->pull_frac > 0 && e->d_P && !e->h_hcache ? e->pull_frac * (double)e->m : 0.0;
     k_plan<<<1, 1024, 0, st>>>(e->nc, e->d_cv0, e->n, e->d_cnt, e->d_cmode, list_frac, max_passes, e->d_wt_type,
                                e->d_wt_prefix, e->d_ctrl, e->d_hubcnt, e->d_log, e->log_cap, cond, use_cond,
                                pull_edges);
@@ -1648,7 +1670,8 @@ static int solve_impl(excent_engine* e, double list_frac, int max_passes, int us
     EX_CHECK_ARG(e, "null engine");
     EX_CHECK_ARG(max_passes >= 0 && max_passes < e->log_cap, "max_passes must be < %d", e->log_cap);
     for (int c = 0; c < e->nc; c++)
-        EX_CHECK_ARG(e->loaded[c], "chunk %d is not loaded in the edge cache (device solve needs every chunk cached)", c);
+        EX_CHECK_ARG(e->loaded[c] || (e->h_hcache && e->ce[c] >= e->cache_edges),
+                     "chunk %d is neither in the edge cache nor in the host cache", c);
     EX_CUDA(cudaSetDevice(e->dev));
     std::vector<uint8_t> cm(e->nc, 1);
     EX_CUDA(cudaMemcpyAsync(e->d_cmode, cm.data(), e->nc, cudaMemcpyHostToDevice, e->s_main));
@@ -1837,6 +1860,34 @@ extern "C" int excent_engine_set_hub_order(excent_engine* e, int first) {
     EX_CUDA(cudaSetDevice(e->dev));
     invalidate_graph(e);
     e->hubs_first = first != 0;
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_host_cache(excent_engine* e, int32_t** host_edges, unsigned long long* first_edge) {
+    EX_CHECK_ARG(e && host_edges, "null argument");
+    EX_CUDA(cudaSetDevice(e->dev));
+    invalidate_graph(e);
+    EX_CUDA(cudaDeviceSynchronize());
+    if (e->h_hcache) { cudaFreeHost(e->h_hcache); e->h_hcache = nullptr; e->hcache_edges = 0; }
+    *host_edges = nullptr;
+    const ull cnt = e->m - e->cache_edges;
+    if (first_edge) *first_edge = e->cache_edges;
+    if (cnt == 0) return EXCENT_OK;
+    if (cudaHostAlloc((void**)&e->h_hcache, cnt * sizeof(int), cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();
+        e->h_hcache = nullptr;
+        EX_FAIL(EXCENT_ERR_NOMEM, "pinned host cache of %llu entries does not fit", cnt);
+    }
+    e->hcache_edges = cnt;
+    *host_edges = e->h_hcache;
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_host_pushed(excent_engine* e, unsigned long long* entries) {
+    EX_CHECK_ARG(e && entries, "null argument");
+    EX_CUDA(cudaSetDevice(e->dev));
+    EX_CUDA(cudaStreamSynchronize(e->s_main));
+    EX_CUDA(cudaMemcpy(entries, &e->d_ctrl->host_pushed, sizeof(ull), cudaMemcpyDeviceToHost));
     return EXCENT_OK;
 }
 

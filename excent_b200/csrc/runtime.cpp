@@ -44,6 +44,7 @@ struct Options {
     bool ev_init_fp64 = false; // eigenvector initial residual from the FP64 lambda1
     int hub_targets = -1;      // shared-memory aggregation of the top-degree targets (-1: auto)
     bool hub_first = true;     // device loop: push the high-degree lists first in every pass
+    std::string host_cache = "off";   // pinned: entries past the HBM cache read in place from pinned host memory
 };
 
 static const char* USAGE =
@@ -106,6 +107,12 @@ static int parse_options(int argc, char** argv, Options& o) {
                 else if (!strcmp(v, "off")) o.hub_targets = 0;
                 else o.hub_targets = atoi(v);
                 if (o.hub_targets < -1) { fprintf(stderr, "--hub-targets must be auto, off or a count\n"); return 1; }
+            }
+        }
+        else if (a == "--host-cache") {
+            if ((ok = next(v))) {
+                if (strcmp(v, "pinned") && strcmp(v, "off")) { fprintf(stderr, "--host-cache must be pinned or off\n"); return 1; }
+                o.host_cache = v;
             }
         }
         else if (a == "--hub-first") {
@@ -214,6 +221,7 @@ static int run(const Options& o) {
         return f;
     };
     if (free_mem()) return 1;
+    if (o.host_cache == "pinned") cache_mode = "chunks";   // an HBM chunk prefix, the rest in host memory
     if (cache_mode == "auto") {   // src/excent.cu:402-409
         const ull freeB = avail_free();
         const bool fits = freeB > reserve && m * sizeof(int) <= freeB - reserve;
@@ -343,12 +351,25 @@ static int run(const Options& o) {
     }
 
     // --device-loop on a fully cached graph: load every chunk now and run the on-device pass loop
-    const bool dev_loop = o.device_loop && cache_mode == "chunks" && n_resident == nc && !hot_mode;
+    // --host-cache pinned: the chunks past the HBM prefix are read once into pinned host memory and
+    // the on-device pass loop pushes from there in place
+    const bool host_loop = o.host_cache == "pinned" && !hot_mode;
+    const bool dev_loop = (o.device_loop && cache_mode == "chunks" && n_resident == nc && !hot_mode) || host_loop;
+    ull host_gb_edges = 0;
     if (dev_loop) {
-        for (int c = 0; c < nc; c++) {
+        for (int c = 0; c < n_resident; c++) {
             RT_CK(g.read_edges(chunks[c].e0, chunks[c].e1, s_edges[0]));
             RT_CK(excent_engine_load_cache(e, chunks[c].e0, chunks[c].e1, s_edges[0]));
             loaded[c] = 1;
+        }
+        if (host_loop) {
+            int32_t* h = nullptr;
+            ull first = 0;
+            RT_CK(excent_engine_host_cache(e, &h, &first));
+            if (h) RT_CK(g.read_edges(first, m, h));
+            host_gb_edges = m - first;
+            printf("host cache: pinned, %.2f GB (%d chunks past the GPU cache), lists read in place over the host link\n",
+                   host_gb_edges * 4.0 / 1e9, nc - n_resident);
         }
     }
     RT_CK(excent_engine_sync(e));
@@ -401,6 +422,11 @@ static int run(const Options& o) {
         std::vector<excent_pass_log> log(std::min(o.max_passes, 1 << 17) + 1);
         RT_CK(excent_engine_stats(e, &st, log.data(), (int)log.size()));
         pass = st.passes;
+        if (host_loop) {   // the lists read in place are this mode's gathered bytes
+            ull hp = 0;
+            RT_CK(excent_engine_host_pushed(e, &hp));
+            bytes_gather += hp * 4;
+        }
         for (int p = 0; p < pass && p < (int)log.size(); p++)
             printf("pass %3d: pending %llu v, demand ratio %.4f | resident %d stream %d gather %d | cached high-degree "
                    "pending %llu | faults major %ld minor %ld | gather pages %llu runs %llu\n",

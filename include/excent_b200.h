@@ -231,6 +231,17 @@ int excent_engine_set_hub_targets(excent_engine* e, int k);
  * default. No reference counterpart (the reference pushes chunk by chunk). */
 int excent_engine_set_hub_order(excent_engine* e, int first);
 
+/* Host cache for graphs larger than device memory: pinned, device-mapped host
+ * memory for the entries past the HBM edge cache (entries [*first_edge, m),
+ * *first_edge = the reserved cache size). The caller fills it (e.g. with
+ * excent_egr_read_edges) before the next excent_engine_solve, whose push
+ * kernels then read those lists in place over the host link (zero copy):
+ * only the lists of pending vertices cross it, with no host-side gather or
+ * staging copy. Reserving the edge cache again frees it. */
+int excent_engine_host_cache(excent_engine* e, int32_t** host_edges, unsigned long long* first_edge);
+/* Entries pushed from the host cache since the last init (4 bytes each crossed the link). */
+int excent_engine_host_pushed(excent_engine* e, unsigned long long* entries);
+
 /* Direction-optimised passes for the device solve on a SYMMETRIC graph (every
  * edge stored in both directions): a pass whose pending demand (sum of
  * pending degrees) is at least pull_frac * m runs as a gather. It takes every

@@ -127,7 +127,7 @@ def test_device_fp64_ppr_matches_cpu_oracle(dgraph):
     for q in queries(n, 3, 11, max_size=200):
         x, it = X.ppr_fp64(n, di, da, q, (1 - d) / len(q), d=d, tol=1e-13)
         t = np.zeros(n)
-        t[q] = 1.0 / len(q)
+        t[q] = float(np.float32((1 - d) / len(q))) / (1 - d)   # the seed value as float32, like the device's
         ref = O.ppr(n, idx, adj, t, kind=0, d=d)
         assert it > 10
         assert np.abs(x - ref).max() <= 1e-10 * max(ref.max(), 1e-30) + 1e-14

@@ -419,3 +419,50 @@ def test_high_degree_first_order(rmat16, measure, use_graph, pull):
     for mode in ("first", "first+targets"):
         for name in names:
             assert res[(mode, name)]["l1_rel"] <= 1.25 * res[("plain", name)]["l1_rel"] + 1e-5, (mode, name, res)
+
+
+@pytest.mark.parametrize("measure", ["pr", "all"])
+@pytest.mark.parametrize("use_graph", [True, False])
+@pytest.mark.parametrize("resident", [0, 2])
+def test_host_cache_zero_copy_solve(rmat16, measure, use_graph, resident):
+    """Chunks past the HBM cache read in place from pinned host memory: the
+    device solve reaches the fixed point of the fully cached solve, and the
+    entries it pushed from host memory are counted."""
+    n, idx, adj = rmat16
+    par = O.params(n, idx, adj)
+    kw = dict(alpha=0.9 / par["_lambda"], lam=par["_lambda"], eps_katz=1e-5, eps_ev=1e-5) if measure == "all" else {}
+    names = ["pr", "katz", "ev"] if measure == "all" else ["pr"]
+    m = len(adj)
+    cap = m // 5 + 1
+    v0, e = chunks_for(idx, cap)
+    assert len(v0) >= 4
+    res = {}
+    for mode in ("device", "host"):
+        meas = X.measures(measure, **kw)
+        eng = X.Engine(n, m, meas, v0, e)
+        eng.upload_offsets(idx)
+        if mode == "device":
+            eng.reserve_cache(m)
+            eng.load_cache(0, m, np.ascontiguousarray(adj, dtype=np.int32))
+        else:
+            ce = int(e[resident])
+            eng.reserve_cache(ce)
+            if ce:
+                eng.load_cache(0, ce, np.ascontiguousarray(adj[:ce], dtype=np.int32))
+            buf, first = eng.host_cache()
+            assert first == ce and len(buf) == m - ce
+            buf[:] = adj[ce:]
+        st = eng.solve(use_graph=use_graph)
+        for i, name in enumerate(names):
+            r = eng.read(i, residual=True)
+            assert np.all(np.abs(r) <= np.float32(meas.eps[i]))
+            ref = O.reference_solution(n, idx, adj, name, alpha=kw.get("alpha"))
+            res[(mode, name)] = O.compare(name, ref, eng.read(i))
+        hp = eng.host_pushed()
+        if mode == "host":
+            assert 0 < hp <= st.pushed
+        else:
+            assert hp == 0
+        eng.close()
+    for name in names:
+        assert res[("host", name)]["l1_rel"] <= 1.25 * res[("device", name)]["l1_rel"] + 1e-5, (name, res)
