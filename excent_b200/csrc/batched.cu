@@ -79,29 +79,45 @@ __device__ __forceinline__ float take_lane(float* rp, float rv, float eps) {
     return fabsf(rv) > eps ? atomicExch(rp, 0.f) : 0.f;
 }
 
-// Scatter one list nb[0..deg) of weights p (this lane's NV float4 of the row,
-// lanes lane % LPR own float4 j = lane % LPR + LPR * k) into R, RPW rows per step.
-template <int LPR, int NV>
-__device__ __forceinline__ ull scatter_rows(const BArgs& a, uint32_t* nxt, const int* nb, unsigned deg,
-                                            const float4 (&p)[NV], const bool (&act)[NV], int lane) {
-    constexpr int RPW = 32 / LPR;
-    const int sub = lane / LPR, j0 = lane % LPR;
+// Scatter list nb[0..deg) of a pushed row with the lanes over entries: lane i
+// takes entry e0 + i and adds the row's nact active 16-byte groups (indices
+// gi[], weights gp[] in shared memory, the same for every lane) to that
+// target's row, so a warp keeps 32 targets in flight.
+__device__ __forceinline__ ull scatter_lanes(const BArgs& a, uint32_t* nxt, const int* nb, unsigned deg,
+                                             const float4* gp, const int* gi, int nact, int lane) {
     ull upd = 0;
     for (unsigned e0 = 0; e0 < deg; e0 += 32) {
-        const int ul = e0 + lane < deg ? ld_edge(nb + e0 + lane) : -1;
-        const unsigned cnt = min(32u, deg - e0);
-        for (unsigned g = 0; g < cnt; g += RPW) {
-            const int u = __shfl_sync(FULL, ul, (int)g + sub);
-            if (g + sub < cnt) {
-                float4* row = a.R + (size_t)u * a.V;
-#pragma unroll
-                for (int k = 0; k < NV; k++)
-                    if (act[k]) { red_add(row, j0 + LPR * k, p[k]); upd++; }
-                if (j0 == 0) mark(nxt, u);
-            }
+        if (e0 + lane < deg) {
+            const int u = ld_edge(nb + e0 + lane);
+            float4* row = a.R + (size_t)u * a.V;
+            for (int i = 0; i < nact; i++) red_add(row, gi[i], gp[i]);
+            mark(nxt, u);
+            upd += (ull)nact;
         }
     }
     return upd;
+}
+
+// Compact the active groups of a row held by lanes j0 + LPR * k (k < NV) into
+// the warp's shared lists; returns their count (warp-uniform).
+template <int LPR, int NV>
+__device__ __forceinline__ int compact_groups(const float4 (&p)[NV], const bool (&act)[NV], float4* gp, int* gi,
+                                              int lane) {
+    const int j0 = lane % LPR;
+    int base = 0;
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+        const bool on = lane < LPR && act[k];
+        const unsigned b = __ballot_sync(FULL, on);
+        if (on) {
+            const int at = base + __popc(b & ((1u << lane) - 1u));
+            gp[at] = p[k];
+            gi[at] = j0 + LPR * k;
+        }
+        base += __popc(b);
+    }
+    __syncwarp();
+    return base;
 }
 
 // One pass: scan touched words (interleaved over warps), check, take and push.
@@ -111,6 +127,8 @@ __global__ void __launch_bounds__(BB) k_bpass(BArgs a) {
     const int j0 = lane % LPR;
     const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    __shared__ float4 s_gp[BB / 32][LPR * NV];
+    __shared__ int s_gi[BB / 32][LPR * NV];
     const int par = a.ctrl->pass & 1;
     uint32_t* cur = a.touched[par];
     uint32_t* nxt = a.touched[par ^ 1];
@@ -213,7 +231,9 @@ __global__ void __launch_bounds__(BB) k_bpass(BArgs a) {
                 }
                 continue;
             }
-            upd += scatter_rows<LPR, NV>(a, nxt, nb, deg, p, act, lane);
+            const int nact = compact_groups<LPR, NV>(p, act, s_gp[wib], s_gi[wib], lane);
+            upd += scatter_lanes(a, nxt, nb, deg, s_gp[wib], s_gi[wib], nact, lane);
+            __syncwarp();
         }
     }
     __shared__ ull s_v[BB / 32], s_e[BB / 32], s_u[BB / 32], s_c[BB / 32];
@@ -243,6 +263,8 @@ __global__ void __launch_bounds__(BB) k_bhub(BArgs a) {
     uint32_t* nxt = a.touched[par ^ 1];
     ull nseg = a.ctrl->hub_segs[par];
     if (nseg > a.seg_cap) nseg = a.seg_cap;
+    __shared__ float4 s_gp[BB / 32][LPR * NV];
+    __shared__ int s_gi[BB / 32][LPR * NV];
     ull upd = 0;
     for (long long s = gw; s < (long long)nseg; s += nwarps) {
         const BSeg sg = a.seg[s];
@@ -250,10 +272,12 @@ __global__ void __launch_bounds__(BB) k_bhub(BArgs a) {
         bool act[NV];
 #pragma unroll
         for (int k = 0; k < NV; k++) {
-            p[k] = a.P[(size_t)sg.slot * a.V + j0 + LPR * k];
+            p[k] = lane < LPR ? a.P[(size_t)sg.slot * a.V + j0 + LPR * k] : make_float4(0.f, 0.f, 0.f, 0.f);
             act[k] = nonzero(p[k]);
         }
-        upd += scatter_rows<LPR, NV>(a, nxt, sg.nb, sg.len, p, act, lane);
+        const int nact = compact_groups<LPR, NV>(p, act, s_gp[wib], s_gi[wib], lane);
+        upd += scatter_lanes(a, nxt, sg.nb, sg.len, s_gp[wib], s_gi[wib], nact, lane);
+        __syncwarp();
     }
     __shared__ ull s_u[BB / 32];
     upd = warp_sum(upd);

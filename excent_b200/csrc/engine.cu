@@ -826,13 +826,20 @@ __global__ void k_hub_list(int n, const ull* idx, int* out, ull* cnt) {
 }
 
 // Encode / decode the edge cache for hub-target aggregation.
-__global__ void k_hub_encode(ull m, int* adj, const int* slot_of, int n) {
+// hub_id is sorted: a binary search in shared memory gives an entry's slot.
+__global__ void k_hub_encode(ull m, int* adj, const int* hub_id, int hub_k) {
+    extern __shared__ int s_ids[];
+    for (int i = threadIdx.x; i < hub_k; i += blockDim.x) s_ids[i] = hub_id[i];
+    __syncthreads();
     for (ull e = blockIdx.x * (ull)blockDim.x + threadIdx.x; e < m; e += (ull)gridDim.x * blockDim.x) {
         const int u = adj[e];
-        if (u >= 0 && u < n) {
-            const int sl = slot_of[u];
-            if (sl >= 0) adj[e] = (int)(0x80000000u | (unsigned)sl);
+        if (u < 0) continue;
+        int lo = 0, hi = hub_k - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (s_ids[mid] < u) lo = mid + 1; else hi = mid;
         }
+        if (s_ids[lo] == u) adj[e] = (int)(0x80000000u | (unsigned)lo);
     }
 }
 __global__ void k_hub_decode(ull m, int* adj, const int* hub_id, int hub_k) {
@@ -907,7 +914,6 @@ struct excent_engine {
     float* d_v1 = nullptr;   // unit principal eigenvector for the EV normalisation step
     void* d_P = nullptr;     // per-vertex push weights of a pull pass
     int* d_hub_id = nullptr; // hub-target aggregation: vertex of each slot
-    int* d_slot = nullptr;   // slot of each vertex (-1: none), kept to encode later cache loads
     int hub_k = 0;           // slots in use (0: off)
     int* h_hcache = nullptr; // pinned, mapped host copy of the entries past the device cache
     ull hcache_edges = 0;
@@ -964,7 +970,7 @@ static int free_engine(excent_engine* e) {
     cudaDeviceSynchronize();
     if (e->gexec) cudaGraphExecDestroy(e->gexec);
     if (e->graph) cudaGraphDestroy(e->graph);
-    void* dptrs[] = {e->d_hub_id, e->d_slot, e->d_hubv, e->d_hubv_cnt, e->d_P, e->d_v1, e->d_idx, e->d_x, e->d_r, e->d_bitmap, e->d_cnt, e->d_cv0, e->d_list, e->d_ctrl, e->d_cmode,
+    void* dptrs[] = {e->d_hub_id, e->d_hubv, e->d_hubv_cnt, e->d_P, e->d_v1, e->d_idx, e->d_x, e->d_r, e->d_bitmap, e->d_cnt, e->d_cv0, e->d_list, e->d_ctrl, e->d_cmode,
                      e->d_wt_type, e->d_wt_prefix, e->d_hubq[0], e->d_hubq[1], e->d_hubq[2], e->d_hubcnt, e->d_log, e->d_trace, e->d_tmp, e->d_cache,
                      e->d_hids, e->d_hoff, e->d_hedges, e->d_hot, e->d_hlist};
     for (void* p : dptrs) if (p) cudaFree(p);
@@ -1065,8 +1071,9 @@ static int engine_setup(excent_engine* e, int device, int n, ull m, const excent
 
 // Encode cache entries [e0, e1) for hub-target aggregation (no-op when off).
 static void hub_encode(excent_engine* e, ull e0, ull e1, cudaStream_t st) {
-    if (!e->hub_k || !e->d_slot || e1 <= e0) return;
-    k_hub_encode<<<e->sms * 8, BLOCK, 0, st>>>(e1 - e0, e->d_cache + e0, e->d_slot, e->n);
+    if (!e->hub_k || e1 <= e0) return;
+    k_hub_encode<<<e->sms * 4, BLOCK, (size_t)e->hub_k * sizeof(int), st>>>(e1 - e0, e->d_cache + e0, e->d_hub_id,
+                                                                            e->hub_k);
     e->launches++;
 }
 
@@ -1156,7 +1163,6 @@ extern "C" int excent_engine_reserve_cache(excent_engine* e, unsigned long long 
     EX_CUDA(cudaDeviceSynchronize());
     if (e->d_cache) { cudaFree(e->d_cache); e->d_cache = nullptr; e->cache_edges = 0; }
     e->hub_k = 0;   // a fresh cache holds plain ids
-    if (e->d_slot) { cudaFree(e->d_slot); e->d_slot = nullptr; }
     if (e->h_hcache) { cudaFreeHost(e->h_hcache); e->h_hcache = nullptr; e->hcache_edges = 0; }
     if (edges == 0) return EXCENT_OK;
     if (cudaMalloc((void**)&e->d_cache, edges * sizeof(int)) != cudaSuccess) {
@@ -1832,20 +1838,13 @@ extern "C" int excent_engine_set_hub_targets(excent_engine* e, int k) {
         });
         ids.resize(k);
         std::sort(ids.begin(), ids.end());
-        std::vector<int> slot_of(e->n, -1);
-        for (int i = 0; i < k; i++) slot_of[ids[i]] = i;
         if (!e->d_hub_id) EX_ALLOC(e->d_hub_id, (size_t)kmax * sizeof(int));
-        if (!e->d_slot) EX_ALLOC(e->d_slot, (size_t)e->n * sizeof(int));
         EX_CUDA(cudaMemcpy(e->d_hub_id, ids.data(), (size_t)k * sizeof(int), cudaMemcpyHostToDevice));
-        EX_CUDA(cudaMemcpy(e->d_slot, slot_of.data(), (size_t)e->n * sizeof(int), cudaMemcpyHostToDevice));
         e->hub_k = k;
         for (int c = 0; c < e->nc; c++)   // chunks loaded so far; later loads encode themselves
             if (e->loaded[c] && e->ce[c + 1] <= e->cache_edges) hub_encode(e, e->ce[c], e->ce[c + 1], e->s_main);
         EX_CUDA(cudaStreamSynchronize(e->s_main));
         EX_CUDA(cudaGetLastError());
-    } else if (e->d_slot) {
-        cudaFree(e->d_slot);
-        e->d_slot = nullptr;
     }
     const size_t smem = hub_smem(e);
     int occ = 0;

@@ -63,7 +63,7 @@ MODES = {
     "zero-copy": ["--stream-ratio", "0.3", "--cache", "none", "--zero-copy", "on", "--chunk-medges", "0.02"],
     "device-loop": ["--stream-ratio", "2", "--cache", "chunks", "--device-loop"],
     "nodedup": ["--stream-ratio", "2", "--cache", "none", "--dedup", "off", "--chunk-medges", "0.05"],
-    "host-cache": ["--stream-ratio", "2", "--host-cache", "pinned", "--chunk-medges", "0.02", "--gpu-budget-gb", "0.0012",
+    "host-cache": ["--stream-ratio", "2", "--host-cache", "pinned", "--chunk-medges", "0.02", "--gpu-budget-gb", "0.0004",
                    "--reserve-mb", "0"],
 }
 
@@ -80,7 +80,7 @@ def test_cli_modes_vs_oracle(rmat14, tmp_path, mode, measure):
     if mode in ("gather", "mixed", "nodedup"):
         assert re.search(r"gather [1-9]", out), out
     if mode == "host-cache":
-        assert "host cache: pinned" in out
+        assert re.search(r"host cache: pinned, [0-9.]+ GB \([1-9]\d* chunks past the GPU cache\)", out), out
         assert re.search(r"gather [0-9.]*[1-9][0-9.]* GB", out), out
     if mode.startswith("hot"):
         assert "GPU degree cache:" in out
