@@ -99,6 +99,7 @@ PROTOS = [
                                           f64p]),
     ("excent_wgraph_grad_fp64", C.c_int, [vp, C.c_int, C.c_double, vp, vp, C.c_double, vp, vp]),
     ("excent_wgraph_stream", C.c_int, [vp, C.POINTER(vp)]),
+    ("excent_wgraph_host_transposed", C.c_int, [vp]),
     ("excent_params_fp64", C.c_int, [C.c_int, C.c_int, vp, vp, C.c_double, f64p, vp]),
     ("excent_engine_ev_project", C.c_int, [vp, vp]),
     ("excent_engine_set_pull", C.c_int, [vp, C.c_double]),

@@ -36,6 +36,10 @@ class WeightedGraph:
         self._w = w.detach().contiguous().float()
         call("excent_wgraph_set_weights", self.h, self._w.data_ptr())
 
+    def host_transposed(self):
+        """Keep the transposed graph in pinned host memory, read in place by the adjoint push."""
+        call("excent_wgraph_host_transposed", self.h)
+
     def close(self):
         if self.h:
             call("excent_wgraph_destroy", self.h)

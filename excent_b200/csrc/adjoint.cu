@@ -271,6 +271,10 @@ struct excent_wgraph {
     float geps[2] = {-1, -1}, gs[2] = {0, 0};
     int grid = 0;
     bool have_fwd = false;
+    bool host_t = false;          // transposed lists and weights in pinned, mapped host memory
+    int* h_adjT = nullptr;
+    float* h_wt = nullptr;
+    double* h_wt64 = nullptr;
     int fwd_kind = -1;
     double fwd_s = 0;
     ull launches = 0;
@@ -290,6 +294,12 @@ static void wg_free(excent_wgraph* g) {
     cudaSetDevice(g->dev);
     cudaDeviceSynchronize();
     wg_drop_graphs(g);
+    if (g->host_t) {
+        cudaFreeHost(g->h_adjT);
+        cudaFreeHost(g->h_wt);
+        cudaFreeHost(g->h_wt64);
+        g->d_adjT = nullptr; g->d_wt = nullptr; g->d_wt64 = nullptr;
+    }
     void* ps[] = {g->d_wn, g->d_wn64, g->d_rowsum, g->d_idxT, g->d_adjT, g->d_perm, g->d_inv, g->d_wt, g->d_wt64,
                   g->d_x, g->d_r, g->d_lam, g->d_t[0], g->d_t[1], g->d_ctrl, g->d_v64[0], g->d_v64[1], g->d_mx,
                   g->d_red};
@@ -575,7 +585,7 @@ static int wg_perturb(excent_wgraph* g, long long e, double delta, int* u_out, s
     EX_CUDA(cudaMemcpy(g->d_wn64 + b, q.data(), d * 8, cudaMemcpyHostToDevice));
     std::vector<unsigned> inv(d);
     EX_CUDA(cudaMemcpy(inv.data(), g->d_inv + b, d * 4, cudaMemcpyDeviceToHost));
-    for (ull i = 0; i < d; i++) EX_CUDA(cudaMemcpy(g->d_wt64 + inv[i], &q[i], 8, cudaMemcpyHostToDevice));
+    for (ull i = 0; i < d; i++) EX_CUDA(cudaMemcpy(g->d_wt64 + inv[i], &q[i], 8, cudaMemcpyDefault));
     *u_out = u;
     return EXCENT_OK;
 }
@@ -587,7 +597,7 @@ static int wg_restore(excent_wgraph* g, int u, const std::vector<double>& saved)
     EX_CUDA(cudaMemcpy(g->d_wn64 + b[0], saved.data(), d * 8, cudaMemcpyHostToDevice));
     std::vector<unsigned> inv(d);
     EX_CUDA(cudaMemcpy(inv.data(), g->d_inv + b[0], d * 4, cudaMemcpyDeviceToHost));
-    for (ull i = 0; i < d; i++) EX_CUDA(cudaMemcpy(g->d_wt64 + inv[i], &saved[i], 8, cudaMemcpyHostToDevice));
+    for (ull i = 0; i < d; i++) EX_CUDA(cudaMemcpy(g->d_wt64 + inv[i], &saved[i], 8, cudaMemcpyDefault));
     return EXCENT_OK;
 }
 
@@ -644,5 +654,40 @@ extern "C" int excent_wgraph_grad_fp64(excent_wgraph* g, int kind, double s, con
 extern "C" int excent_wgraph_stream(excent_wgraph* g, void** stream) {
     EX_CHECK_ARG(g && stream, "null argument");
     *stream = (void*)g->st;
+    return EXCENT_OK;
+}
+
+// Move the transposed lists and weights to pinned, device-mapped host memory:
+// the adjoint push then reads them in place over the host link (zero copy),
+// the way the engine's host cache serves graphs larger than device memory.
+extern "C" int excent_wgraph_host_transposed(excent_wgraph* g) {
+    EX_CHECK_ARG(g, "null graph");
+    if (g->host_t || g->m == 0) return EXCENT_OK;
+    EX_CUDA(cudaSetDevice(g->dev));
+    EX_CUDA(cudaDeviceSynchronize());
+    wg_drop_graphs(g);
+    const unsigned fl = cudaHostAllocMapped | cudaHostAllocPortable;
+    int* ha = nullptr;
+    float* hw = nullptr;
+    double* hw64 = nullptr;
+    if (cudaHostAlloc((void**)&ha, g->m * 4, fl) != cudaSuccess || cudaHostAlloc((void**)&hw, g->m * 4, fl) != cudaSuccess ||
+        cudaHostAlloc((void**)&hw64, g->m * 8, fl) != cudaSuccess) {
+        cudaGetLastError();
+        if (ha) cudaFreeHost(ha);
+        if (hw) cudaFreeHost(hw);
+        if (hw64) cudaFreeHost(hw64);
+        EX_FAIL(EXCENT_ERR_NOMEM, "pinned host copy of the transposed graph does not fit");
+    }
+    EX_CUDA(cudaMemcpy(ha, g->d_adjT, g->m * 4, cudaMemcpyDeviceToHost));
+    EX_CUDA(cudaMemcpy(hw, g->d_wt, g->m * 4, cudaMemcpyDeviceToHost));
+    EX_CUDA(cudaMemcpy(hw64, g->d_wt64, g->m * 8, cudaMemcpyDeviceToHost));
+    cudaFree(g->d_adjT);
+    cudaFree(g->d_wt);
+    cudaFree(g->d_wt64);
+    g->h_adjT = ha; g->h_wt = hw; g->h_wt64 = hw64;
+    EX_CUDA(cudaHostGetDevicePointer((void**)&g->d_adjT, ha, 0));
+    EX_CUDA(cudaHostGetDevicePointer((void**)&g->d_wt, hw, 0));
+    EX_CUDA(cudaHostGetDevicePointer((void**)&g->d_wt64, hw64, 0));
+    g->host_t = true;
     return EXCENT_OK;
 }

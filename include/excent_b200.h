@@ -431,6 +431,11 @@ int excent_wgraph_loss_fp64(excent_wgraph* g, int kind, double s, const float* d
 int excent_wgraph_grad_fp64(excent_wgraph* g, int kind, double s, const float* d_t, const float* d_c, double tol,
                             double* grad_t, double* grad_w);
 int excent_wgraph_stream(excent_wgraph* g, void** stream);
+/* Out of core: move the transposed lists and their weights (4 + 4 + 8 bytes
+ * per entry) to pinned, device-mapped host memory; the adjoint push then
+ * reads them in place over the host link, the way excent_engine_host_cache
+ * serves the plain engine. Irreversible for this graph. */
+int excent_wgraph_host_transposed(excent_wgraph* g);
 
 /* ------------------------------------------------------------ FP64 tools */
 

@@ -130,3 +130,36 @@ def test_katz_beta_gradient(wg):
     lam = O.weighted_adjoint(idx, adj, wn, 0.7, c)
     g = beta.grad.cpu().numpy()
     assert np.linalg.norm(g - lam) <= 1e-4 * np.linalg.norm(lam)
+
+
+def test_vjp_with_the_transposed_graph_in_host_memory():
+    """The adjoint reads the transposed lists in place from pinned host memory
+    and gives the gradients of the device-resident run (and of the oracle)."""
+    g = X.DeviceGraph(12, 16, 4, symmetric=False, weights=True)
+    idx, adj, w = g.download()
+    m = g.m
+    dev = torch.device("cuda")
+    t_idx = torch.from_numpy(idx.view(np.int64)).to(dev)
+    t_adj = torch.from_numpy(adj[:m].copy()).to(dev)
+    t_w = torch.from_numpy(w[:m].copy()).to(dev)
+    n = g.n
+    c = np.zeros(n, dtype=np.float32)
+    c[targets(n)] = 1
+    res = []
+    for host in (False, True):
+        G = WeightedGraph(n, t_idx, t_adj, t_w)
+        if host:
+            G.host_transposed()
+        G.forward("pr", 0.85, None, 1e-7)
+        gt, gw = G.vjp(torch.from_numpy(c).cuda(), 1e-7)
+        res.append((gt.cpu().numpy(), gw.cpu().numpy()))
+        G.close()
+    (gt0, gw0), (gt1, gw1) = res
+    assert np.linalg.norm(gt1 - gt0) <= 1e-4 * np.linalg.norm(gt0)
+    assert np.linalg.norm(gw1 - gw0) <= 1e-4 * np.linalg.norm(gw0)
+    wn = O.row_normalise(idx, w[:m])
+    x_ref = O.weighted_forward(idx, adj[:m], wn, 0.15, 0.85, np.ones(n))
+    lam_ref = O.weighted_adjoint(idx, adj[:m], wn, 0.85, c.astype(np.float64))
+    gw_ref = O.weighted_grad(idx, adj[:m], w[:m], wn, 0.85, x_ref, lam_ref)
+    assert np.linalg.norm(gw1 - gw_ref) <= 1e-3 * np.linalg.norm(gw_ref)
+    g.close()
