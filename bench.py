@@ -349,7 +349,7 @@ def run_ppr(a, world, rank, local, dist):
     ev0.record(st)
     tot_e = 0
     passes = []
-    counters = {"pushed_vertices": 0, "lane_updates": 0, "rows_checked": 0}
+    counters = {"pushed_vertices": 0, "lane_updates": 0, "rows_checked": 0, "hub_segments": 0}
     for i in range(0, len(qs), best):
         b.seed(qs[i:i + best], vals[i:i + best], eps)
         s = b.solve()

@@ -387,10 +387,10 @@ class Batch:
 
     def stats(self):
         p = C.c_int()
-        v, e, u, c = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint64()
-        call("excent_batch_stats", self.h, C.byref(p), C.byref(v), C.byref(e), C.byref(u), C.byref(c))
+        v, e, u, c, hs = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint64()
+        call("excent_batch_stats", self.h, C.byref(p), C.byref(v), C.byref(e), C.byref(u), C.byref(c), C.byref(hs))
         return {"passes": p.value, "pushed_vertices": v.value, "pushed_edges": e.value, "lane_updates": u.value,
-                "rows_checked": c.value}
+                "rows_checked": c.value, "hub_segments": hs.value}
 
     def read(self, lane, residual=False, out=None):
         if out is None:

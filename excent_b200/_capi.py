@@ -72,7 +72,7 @@ PROTOS = [
     ("excent_batch_destroy", C.c_int, [vp]),
     ("excent_batch_seed", C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
     ("excent_batch_solve", C.c_int, [vp, C.c_int, C.c_int]),
-    ("excent_batch_stats", C.c_int, [vp, C.POINTER(C.c_int), u64p, u64p, u64p, u64p]),
+    ("excent_batch_stats", C.c_int, [vp, C.POINTER(C.c_int), u64p, u64p, u64p, u64p, u64p]),
     ("excent_batch_read", C.c_int, [vp, C.c_int, C.c_int, vp]),
     ("excent_batch_stream", C.c_int, [vp, C.POINTER(vp)]),
     ("excent_batch_launches", C.c_int, [vp, u64p]),

@@ -46,6 +46,7 @@ struct BCtrl {
     ull hub_rows[2], hub_segs[2];
     ull total_v, total_e, total_lane_e;  // totals over the solve
     ull rows_checked;                    // touched rows examined, over the solve
+    ull total_segs;                      // hub segments queued, over the solve
     int err;
     int done;
 };
@@ -295,6 +296,7 @@ __global__ void k_bend(BCtrl* c, cudaGraphConditionalHandle cond, int use_cond) 
     const int par = c->pass & 1;
     const ull pv = c->pushed_v[par];
     c->total_v += pv;
+    c->total_segs += c->hub_segs[par];
     c->pushed_v[par ^ 1] = 0;
     c->hub_rows[par ^ 1] = 0;
     c->hub_segs[par ^ 1] = 0;
@@ -556,7 +558,7 @@ extern "C" int excent_batch_solve(excent_batch* b, int max_passes, int use_graph
 
 extern "C" int excent_batch_stats(excent_batch* b, int* passes, unsigned long long* pushed_vertices,
                                   unsigned long long* pushed_edges, unsigned long long* lane_updates,
-                                  unsigned long long* rows_checked) {
+                                  unsigned long long* rows_checked, unsigned long long* hub_segments) {
     EX_CHECK_ARG(b, "null batch");
     EX_CUDA(cudaSetDevice(b->dev));
     BCtrl c;
@@ -567,6 +569,7 @@ extern "C" int excent_batch_stats(excent_batch* b, int* passes, unsigned long lo
     if (pushed_edges) *pushed_edges = c.total_e;
     if (lane_updates) *lane_updates = c.total_lane_e;
     if (rows_checked) *rows_checked = c.rows_checked;
+    if (hub_segments) *hub_segments = c.total_segs;
     return EXCENT_OK;
 }
 

@@ -821,7 +821,7 @@ __global__ void k_hub_list(int n, const ull* idx, int* out, ull* cnt) {
         ull base = 0;
         if (lane == 0) base = atomicAdd(cnt, (ull)__popc(b));
         base = __shfl_sync(FULL, base, 0);
-        if (h) out[base + __popc(b & ((1u << lane) - 1u))] = (int)v;
+        if (h && out) out[base + __popc(b & ((1u << lane) - 1u))] = (int)v;
     }
 }
 
@@ -919,6 +919,7 @@ struct excent_engine {
     ull hcache_edges = 0;
     int* d_hubv = nullptr;   // high-degree-first order: vertices with lists longer than HUB_MIN
     ull* d_hubv_cnt = nullptr;
+    ull hubv_cap = 0;
     bool hubs_first = true;
     bool hubv_stale = true;
     double pull_frac = 0;    // pull when the pending demand >= pull_frac * m (0: never)
@@ -1563,7 +1564,8 @@ static void enqueue_pass(excent_engine* e, double list_frac, int max_passes, cud
     if (ev) cudaEventRecord(ev[2], st);
     PushArgs a = push_args(e, 0);
     const int gt = e->sms * 8;
-    if (e->hubs_first) {
+    const bool hubs_first = e->hubs_first && e->d_hubv && !e->hubv_stale;
+    if (hubs_first) {
         // the high-degree lists first, so their (large) share of the pass's residual reaches
         // every other vertex before that vertex is taken
         if (e->L == 1) k_push<1, SRC_HUBS><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
@@ -1590,7 +1592,7 @@ static void enqueue_pass(excent_engine* e, double list_frac, int max_passes, cud
         e->launches += 2;
     }
     if (ev) cudaEventRecord(ev[3], st);
-    if (!e->hubs_first) {   // with the high-degree lists first, the table push queues no segments
+    if (!hubs_first) {   // with the high-degree lists first, the table push queues no segments
         if (e->L == 1) k_hub<1><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
         else k_hub<4><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
         e->launches++;
@@ -1683,24 +1685,41 @@ static int solve_impl(excent_engine* e, double list_frac, int max_passes, int us
     EX_CUDA(cudaMemcpyAsync(e->d_cmode, cm.data(), e->nc, cudaMemcpyHostToDevice, e->s_main));
     if (init) EX_TRY(init_state(e));
     else EX_TRY(reset_counters(e));
-    if (e->hubs_first && !e->d_hubv) {
-        EX_ALLOC(e->d_hubv, (size_t)e->n * sizeof(int));
-        EX_ALLOC(e->d_hubv_cnt, sizeof(ull));
-        e->hubv_stale = true;
-    }
     if (e->hubs_first && e->hubv_stale) {
+        // count the high-degree vertices, then list them in a buffer of that size
+        if (!e->d_hubv_cnt) EX_ALLOC(e->d_hubv_cnt, sizeof(ull));
         EX_CUDA(cudaMemsetAsync(e->d_hubv_cnt, 0, sizeof(ull), e->s_main));
-        k_hub_list<<<e->sms * 8, BLOCK, 0, e->s_main>>>(e->n, e->d_idx, e->d_hubv, e->d_hubv_cnt);
-        e->launches++;
-        EX_CUDA(cudaGetLastError());
-        e->hubv_stale = false;
+        k_hub_list<<<e->sms * 8, BLOCK, 0, e->s_main>>>(e->n, e->d_idx, nullptr, e->d_hubv_cnt);
+        ull h = 0;
+        EX_CUDA(cudaMemcpyAsync(&h, e->d_hubv_cnt, sizeof(ull), cudaMemcpyDeviceToHost, e->s_main));
+        EX_CUDA(cudaStreamSynchronize(e->s_main));
+        if (h > e->hubv_cap || !e->d_hubv) {
+            invalidate_graph(e);
+            if (e->d_hubv) cudaFree(e->d_hubv);
+            e->d_hubv = nullptr;
+            e->hubv_cap = 0;
+            if (cudaMalloc((void**)&e->d_hubv, std::max<ull>(h, 1) * sizeof(int)) != cudaSuccess) {
+                cudaGetLastError();   // no room: this solve runs in plain order
+                e->d_hubv = nullptr;
+            } else {
+                e->hubv_cap = std::max<ull>(h, 1);
+            }
+        }
+        if (e->d_hubv) {
+            EX_CUDA(cudaMemsetAsync(e->d_hubv_cnt, 0, sizeof(ull), e->s_main));
+            k_hub_list<<<e->sms * 8, BLOCK, 0, e->s_main>>>(e->n, e->d_idx, e->d_hubv, e->d_hubv_cnt);
+            e->launches += 2;
+            EX_CUDA(cudaGetLastError());
+            e->hubv_stale = false;
+        }
     }
     if (use_graph) {
         EX_TRY(build_graph(e, list_frac, max_passes));
         EX_CUDA(cudaGraphLaunch(e->gexec, e->s_main));
         EX_CUDA(cudaStreamSynchronize(e->s_main));
         EX_CUDA(cudaMemcpy(e->h_ctrl, e->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
-        e->launches += ((e->pull_frac > 0 && e->d_P ? 7ull : 4ull) + (e->hubs_first ? 1ull : 0ull)) * (e->h_ctrl->pass + 1);
+        e->launches += ((e->pull_frac > 0 && e->d_P ? 7ull : 4ull) + (e->hubs_first && e->d_hubv ? 1ull : 0ull)) *
+                       (e->h_ctrl->pass + 1);
     } else {
         for (int p = 0; p <= max_passes; p++) {
             enqueue_pass(e, list_frac, max_passes, 0, 0, e->s_main, e->prof ? e->ev : nullptr);

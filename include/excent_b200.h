@@ -370,11 +370,11 @@ int excent_batch_seed(excent_batch* b, int nq, const int* lane_off, const int32_
  * use_graph all passes run as one CUDA graph with a conditional while node. */
 int excent_batch_solve(excent_batch* b, int max_passes, int use_graph);
 /* Passes, pushed vertices, pushed adjacency entries, 16-byte lane-group
- * reductions issued and touched rows examined by the last solve (any output
- * may be NULL). */
+ * reductions issued, touched rows examined and segments of lists longer than
+ * 2048 entries queued by the last solve (any output may be NULL). */
 int excent_batch_stats(excent_batch* b, int* passes, unsigned long long* pushed_vertices,
                        unsigned long long* pushed_edges, unsigned long long* lane_updates,
-                       unsigned long long* rows_checked);
+                       unsigned long long* rows_checked, unsigned long long* hub_segments);
 /* Values (or residuals) of lane q for all n vertices, to host float32. */
 int excent_batch_read(excent_batch* b, int lane, int residual, float* out);
 int excent_batch_stream(excent_batch* b, void** stream);

@@ -131,3 +131,33 @@ def test_device_fp64_ppr_matches_cpu_oracle(dgraph):
         ref = O.ppr(n, idx, adj, t, kind=0, d=d)
         assert it > 10
         assert np.abs(x - ref).max() <= 1e-10 * max(ref.max(), 1e-30) + 1e-14
+
+
+@pytest.mark.parametrize("B,greedy", [(32, False), (128, True), (256, False)])
+def test_batched_ppr_with_hub_segments(B, greedy):
+    """Seeds on the highest-degree vertices push lists longer than 2048 entries
+    (queued as segments): the results still match the device FP64 oracle."""
+    g = X.DeviceGraph(16, 16, 3)
+    n = g.n
+    idx, adj, _ = g.download()
+    deg = np.diff(idx.astype(np.int64))
+    assert deg.max() > 2048
+    top = np.argsort(-deg)[:8].astype(np.int32)
+    d = 0.85
+    eps = 1e-4 * (1 - d)
+    qs = [np.array([v], dtype=np.int32) for v in top] + queries(n, B - 8, 5)
+    di, da, _ = g.device_ptrs()
+    b = X.Batch(n, g.m, di, da, B, "ppr", d)
+    b.set_greedy(greedy)
+    b.seed(qs, [(1 - d) / len(q) for q in qs], eps)
+    b.solve()
+    st = b.stats()
+    assert st["hub_segments"] > 0
+    for q in list(range(8)) + [B - 1]:
+        r = b.read(q, residual=True)
+        assert np.all(np.abs(r) <= np.float32(eps))
+        ref, _ = X.ppr_fp64(n, di, da, qs[q], (1 - d) / len(qs[q]), d=d, tol=1e-12)
+        err = np.abs(b.read(q) - ref).sum()
+        assert err <= 1.1 * np.abs(r.astype(np.float64)).sum() / (1 - d) + 1e-5, (q, err)
+    b.close()
+    g.close()
