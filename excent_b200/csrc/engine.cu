@@ -641,10 +641,17 @@ template <typename T> __device__ __forceinline__ T zero_of();
 template <> __device__ __forceinline__ float zero_of<float>() { return 0.f; }
 template <> __device__ __forceinline__ float4 zero_of<float4>() { return make_float4(0.f, 0.f, 0.f, 0.f); }
 
+// A gather pass walks a static table built once per graph: tiles of whole
+// 32-vertex groups holding about PULL_TILE entries each (lists longer than
+// HUB_MIN excluded), and segments of HUB_SEG entries of those long lists.
+// Every warp gets the same amount of work, with no queue or atomics.
+static constexpr unsigned PULL_TILE = 4096;
+struct PullTile { unsigned g0, ng; };           // groups [g0, g0 + ng) of 32 vertices
+struct PullSeg { ull b; unsigned len; int v; };  // entries [b, b + len) of v's list
+
 template <int L>
 __global__ void __launch_bounds__(BLOCK) k_pull(int n, void* rv, const void* Pv, const ull* idx, const int* cache,
-                                                HubSeg* hubq, ull* hub_cnt, ull hub_cap, Ctrl* ctrl,
-                                                const int* hub_id) {
+                                                const PullTile* tiles, int ntiles, Ctrl* ctrl, const int* hub_id) {
     typedef typename Lane<L>::T T;
     if (!ctrl->pull) return;
     T* r = reinterpret_cast<T*>(rv);
@@ -655,91 +662,80 @@ __global__ void __launch_bounds__(BLOCK) k_pull(int n, void* rv, const void* Pv,
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long tile = gw; tile * 32 < n; tile += nwarps) {
-        const long long v = tile * 32 + lane;
-        ull b = 0, deg = 0;
-        if (v < n) { b = idx[v]; deg = idx[v + 1] - b; }
-        const int* nb = cache + b;
-        const bool large = deg > HUB_MIN;
-        if (large) {
-            const unsigned nseg = (unsigned)((deg + HUB_SEG - 1) / HUB_SEG);
-            const ull base = atomicAdd(hub_cnt, (ull)nseg);
-            if (base + nseg <= hub_cap) {
-                for (unsigned s = 0; s < nseg; s++) {
-                    HubSeg h;
-                    h.nb = nb + (ull)s * HUB_SEG;
-                    h.len = (unsigned)min((ull)HUB_SEG, deg - (ull)s * HUB_SEG);
-                    h.pad = (unsigned)v;
-                    h.p = make_float4(0.f, 0.f, 0.f, 0.f);
-                    hubq[base + s] = h;
-                }
-            } else {
-                atomicExch(&ctrl->err, 1);
-            }
-        }
-        const unsigned ds = large ? 0u : (unsigned)deg;
-        const unsigned nz = __ballot_sync(FULL, ds != 0);
-        if (!nz) continue;
-        // the tile's nonempty lists in lane order, indexed by their rank among them
-        const int rank = __popc(nz & ((1u << lane) - 1u));
-        const unsigned incl = warp_incl_scan(ds, lane);
-        const unsigned tot = __shfl_sync(FULL, incl, 31);
-        const unsigned ex = incl - ds;
-        if (ds) { s_nb[wib][rank] = nb; s_ex[wib][rank] = ex; s_acc[wib][rank] = zero_of<T>(); }
-        __syncwarp();
-        const unsigned le = lane == 31 ? FULL : (2u << lane) - 1u;   // lanes <= this one
-        for (unsigned j0 = 0; j0 < tot; j0 += 32 * UNROLL) {
-            T val[UNROLL];
-            int own[UNROLL], dist[UNROLL];
-            bool last[UNROLL];
+    const unsigned le = lane == 31 ? FULL : (2u << lane) - 1u;   // lanes <= this one
+    for (long long t = gw; t < ntiles; t += nwarps) {
+        const PullTile tl = tiles[t];
+        for (unsigned g = tl.g0; g < tl.g0 + tl.ng; g++) {
+            const long long v = (long long)g * 32 + lane;
+            ull b = 0, deg = 0;
+            if (v < n) { b = idx[v]; deg = idx[v + 1] - b; }
+            const unsigned ds = deg > HUB_MIN ? 0u : (unsigned)deg;   // long lists: segments
+            const unsigned nz = __ballot_sync(FULL, ds != 0);
+            if (!nz) continue;
+            // the group's nonempty lists in lane order, indexed by their rank among them
+            const int rank = __popc(nz & ((1u << lane) - 1u));
+            const unsigned incl = warp_incl_scan(ds, lane);
+            const unsigned tot = __shfl_sync(FULL, incl, 31);
+            const unsigned ex = incl - ds;
+            if (ds) { s_nb[wib][rank] = cache + b; s_ex[wib][rank] = ex; s_acc[wib][rank] = zero_of<T>(); }
+            __syncwarp();
+            for (unsigned j0 = 0; j0 < tot; j0 += 32 * UNROLL) {
+                T val[UNROLL];
+                int own[UNROLL], dist[UNROLL];
+                bool last[UNROLL];
 #pragma unroll
-            for (int k = 0; k < UNROLL; k++) {
-                // window [wb, wb+32) of the concatenated lists: bit i of `starts` marks a list
-                // beginning at entry wb+i; the owner of entry wb is the last list starting at or
-                // before it, so lane i's owner is that one plus the starts in (wb, wb+i].
-                const unsigned wb = j0 + 32 * k;
-                const unsigned j = wb + lane;
-                const unsigned starts = __reduce_or_sync(FULL, (ds && ex >= wb && ex - wb < 32) ? 1u << (ex - wb) : 0u);
-                const int o0 = __popc(__ballot_sync(FULL, ds && ex <= wb)) - 1;
-                const unsigned sl = starts & le;
-                own[k] = o0 + __popc(sl & ~1u);
-                dist[k] = sl ? lane - (31 - __clz(sl)) : lane;
-                last[k] = j < tot && (lane == 31 || j + 1 == tot || ((starts >> (lane + 1)) & 1u));
-                val[k] = zero_of<T>();
-                if (j < tot) {
-                    int u = ld_edge(s_nb[wib][own[k]] + (j - s_ex[wib][own[k]]));
-                    if (u < 0) u = hub_id[u & HUB_MASK];
-                    val[k] = __ldg(P + u);
+                for (int k = 0; k < UNROLL; k++) {
+                    // window [wb, wb+32) of the concatenated lists: bit i of `starts` marks a list
+                    // beginning at entry wb+i; the owner of entry wb is the last list starting at or
+                    // before it, so lane i's owner is that one plus the starts in (wb, wb+i].
+                    const unsigned wb = j0 + 32 * k;
+                    const unsigned j = wb + lane;
+                    const unsigned starts =
+                        __reduce_or_sync(FULL, (ds && ex >= wb && ex - wb < 32) ? 1u << (ex - wb) : 0u);
+                    const int o0 = __popc(__ballot_sync(FULL, ds && ex <= wb)) - 1;
+                    const unsigned sl = starts & le;
+                    own[k] = o0 + __popc(sl & ~1u);
+                    dist[k] = sl ? lane - (31 - __clz(sl)) : lane;
+                    last[k] = j < tot && (lane == 31 || j + 1 == tot || ((starts >> (lane + 1)) & 1u));
+                    val[k] = zero_of<T>();
+                    if (j < tot) {
+                        int u = ld_edge(s_nb[wib][own[k]] + (j - s_ex[wib][own[k]]));
+                        if (u < 0) u = hub_id[u & HUB_MASK];
+                        val[k] = __ldg(P + u);
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < UNROLL; k++) {
+                    // segmented inclusive sum: lane i adds the lanes of its own list below it
+                    T sv = val[k];
+#pragma unroll
+                    for (int d = 1; d < 32; d <<= 1) {
+                        const T tv = shfl_up(sv, d);
+                        if (d <= dist[k]) acc_add(sv, tv);
+                    }
+                    if (last[k]) acc_add(s_acc[wib][own[k]], sv);
+                    __syncwarp();
                 }
             }
-#pragma unroll
-            for (int k = 0; k < UNROLL; k++) {
-                // segmented inclusive sum: lane i adds the lanes of its own list below it
-                T sv = val[k];
-#pragma unroll
-                for (int d = 1; d < 32; d <<= 1) {
-                    const T t = shfl_up(sv, d);
-                    if (d <= dist[k]) acc_add(sv, t);
+            if (ds) {
+                const T add = s_acc[wib][rank];
+                if (nonzero(add)) {   // this warp owns v: plain read-modify-write
+                    T cur = r[v];
+                    acc_add(cur, add);
+                    r[v] = cur;
                 }
-                if (last[k]) acc_add(s_acc[wib][own[k]], sv);
-                __syncwarp();
             }
+            __syncwarp();
         }
-        if (ds) {
-            const T add = s_acc[wib][rank];
-            if (nonzero(add)) {
-                T cur = r[v];
-                acc_add(cur, add);
-                r[v] = cur;
-            }
-        }
-        __syncwarp();
     }
 }
 
+// The long lists' segments: one warp sums the weights of a segment's entries
+// and adds the sum to the segment's vertex (segments of one list may run on
+// several warps, hence the reduction).
 template <int L>
-__global__ void __launch_bounds__(BLOCK) k_pullhub(void* rv, const void* Pv, const HubSeg* q, const ull* hub_cnt,
-                                                   ull cap, const Ctrl* ctrl, const int* hub_id) {
+__global__ void __launch_bounds__(BLOCK) k_pullhub(void* rv, const void* Pv, const int* cache, const PullSeg* segs,
+                                                   int nseg, const Ctrl* ctrl, const int* hub_id) {
     typedef typename Lane<L>::T T;
     if (!ctrl->pull) return;
     T* r = reinterpret_cast<T*>(rv);
@@ -747,27 +743,34 @@ __global__ void __launch_bounds__(BLOCK) k_pullhub(void* rv, const void* Pv, con
     const int lane = threadIdx.x & 31;
     const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    ull cnt = *hub_cnt;
-    if (cnt > cap) cnt = cap;
-    for (long long s = gw; s < (long long)cnt; s += nwarps) {
-        const HubSeg h = q[s];
+    for (long long s = gw; s < nseg; s += nwarps) {
+        const PullSeg h = segs[s];
+        const int* nb = cache + h.b;
         T acc = zero_of<T>();
-        const unsigned mis = (unsigned)(((uintptr_t)h.nb >> 2) & 3u);
+        const unsigned mis = (unsigned)(((uintptr_t)nb >> 2) & 3u);
         unsigned head = (4u - mis) & 3u;
         if (head > h.len) head = h.len;
         auto dec = [&](int u) { return u < 0 ? hub_id[u & HUB_MASK] : u; };
-        if (lane < (int)head) acc_add(acc, P[dec(ld_edge(h.nb + lane))]);
-        const int4* body = reinterpret_cast<const int4*>(h.nb + head);
+        if (lane < (int)head) acc_add(acc, __ldg(P + dec(ld_edge(nb + lane))));
+        const int4* body = reinterpret_cast<const int4*>(nb + head);
         const unsigned nbody = (h.len - head) >> 2;
-        for (unsigned i = lane; i < nbody; i += 32) {
+        unsigned i = lane;
+        for (; i + 32 < nbody; i += 64) {   // two 128-bit index loads in flight per lane
+            const int4 e0 = ld_edge4(body + i), e1 = ld_edge4(body + i + 32);
+            const T a0 = __ldg(P + dec(e0.x)), a1 = __ldg(P + dec(e0.y)), a2 = __ldg(P + dec(e0.z)), a3 = __ldg(P + dec(e0.w));
+            const T b0 = __ldg(P + dec(e1.x)), b1 = __ldg(P + dec(e1.y)), b2 = __ldg(P + dec(e1.z)), b3 = __ldg(P + dec(e1.w));
+            acc_add(acc, a0); acc_add(acc, a1); acc_add(acc, a2); acc_add(acc, a3);
+            acc_add(acc, b0); acc_add(acc, b1); acc_add(acc, b2); acc_add(acc, b3);
+        }
+        for (; i < nbody; i += 32) {
             const int4 e = ld_edge4(body + i);
-            const T a0 = P[dec(e.x)], a1 = P[dec(e.y)], a2 = P[dec(e.z)], a3 = P[dec(e.w)];
+            const T a0 = __ldg(P + dec(e.x)), a1 = __ldg(P + dec(e.y)), a2 = __ldg(P + dec(e.z)), a3 = __ldg(P + dec(e.w));
             acc_add(acc, a0); acc_add(acc, a1); acc_add(acc, a2); acc_add(acc, a3);
         }
         const unsigned tail = (h.len - head) & 3u;
-        if (lane < (int)tail) acc_add(acc, P[dec(ld_edge(h.nb + head + nbody * 4 + lane))]);
+        if (lane < (int)tail) acc_add(acc, __ldg(P + dec(ld_edge(nb + head + nbody * 4 + lane))));
         acc = warp_sum(acc);
-        if (lane == 0 && nonzero(acc)) red_add(r, (int)h.pad, acc);
+        if (lane == 0 && nonzero(acc)) red_add(r, h.v, acc);
     }
 }
 
@@ -913,6 +916,10 @@ struct excent_engine {
     float* d_tmp = nullptr;  // n floats for readback of the float4 layout
     float* d_v1 = nullptr;   // unit principal eigenvector for the EV normalisation step
     void* d_P = nullptr;     // per-vertex push weights of a pull pass
+    PullTile* d_ptiles = nullptr;   // static work table of gather passes
+    PullSeg* d_psegs = nullptr;
+    int n_ptiles = 0, n_psegs = 0;
+    bool pull_stale = true;
     int* d_hub_id = nullptr; // hub-target aggregation: vertex of each slot
     int hub_k = 0;           // slots in use (0: off)
     int* h_hcache = nullptr; // pinned, mapped host copy of the entries past the device cache
@@ -971,7 +978,7 @@ static int free_engine(excent_engine* e) {
     cudaDeviceSynchronize();
     if (e->gexec) cudaGraphExecDestroy(e->gexec);
     if (e->graph) cudaGraphDestroy(e->graph);
-    void* dptrs[] = {e->d_hub_id, e->d_hubv, e->d_hubv_cnt, e->d_P, e->d_v1, e->d_idx, e->d_x, e->d_r, e->d_bitmap, e->d_cnt, e->d_cv0, e->d_list, e->d_ctrl, e->d_cmode,
+    void* dptrs[] = {e->d_ptiles, e->d_psegs, e->d_hub_id, e->d_hubv, e->d_hubv_cnt, e->d_P, e->d_v1, e->d_idx, e->d_x, e->d_r, e->d_bitmap, e->d_cnt, e->d_cv0, e->d_list, e->d_ctrl, e->d_cmode,
                      e->d_wt_type, e->d_wt_prefix, e->d_hubq[0], e->d_hubq[1], e->d_hubq[2], e->d_hubcnt, e->d_log, e->d_trace, e->d_tmp, e->d_cache,
                      e->d_hids, e->d_hoff, e->d_hedges, e->d_hot, e->d_hlist};
     for (void* p : dptrs) if (p) cudaFree(p);
@@ -1140,6 +1147,7 @@ extern "C" int excent_engine_upload_offsets(excent_engine* e, const unsigned lon
     EX_CUDA(cudaMemcpyAsync(e->d_idx + v0, idx, count * sizeof(ull), cudaMemcpyHostToDevice, e->s_main));
     EX_CUDA(cudaStreamSynchronize(e->s_main));
     e->hubv_stale = true;
+    e->pull_stale = true;
     return EXCENT_OK;
 }
 
@@ -1153,6 +1161,7 @@ extern "C" int excent_engine_upload_device(excent_engine* e, const unsigned long
     EX_CUDA(cudaStreamSynchronize(e->s_main));
     EX_CUDA(cudaGetLastError());
     e->hubv_stale = true;
+    e->pull_stale = true;
     std::fill(e->loaded.begin(), e->loaded.end(), 1);
     return EXCENT_OK;
 }
@@ -1582,12 +1591,12 @@ static void enqueue_pass(excent_engine* e, double list_frac, int max_passes, cud
     if (pull_edges > 0) {   // each of these returns at once unless k_plan chose a pull pass
         if (e->L == 1) {
             k_take<1><<<gt, BLOCK, 0, st>>>(e->n, e->d_x, e->d_r, e->d_P, e->d_idx, e->M, e->d_ctrl);
-            k_pull<1><<<e->grid_push, BLOCK, 0, st>>>(e->n, e->d_r, e->d_P, e->d_idx, e->d_cache, a.hubq, a.hub_cnt,
-                                                       a.hub_cap, e->d_ctrl, e->d_hub_id);
+            k_pull<1><<<e->grid_push, BLOCK, 0, st>>>(e->n, e->d_r, e->d_P, e->d_idx, e->d_cache, e->d_ptiles,
+                                                       e->n_ptiles, e->d_ctrl, e->d_hub_id);
         } else {
             k_take<4><<<gt, BLOCK, 0, st>>>(e->n, e->d_x, e->d_r, e->d_P, e->d_idx, e->M, e->d_ctrl);
-            k_pull<4><<<e->grid_push, BLOCK, 0, st>>>(e->n, e->d_r, e->d_P, e->d_idx, e->d_cache, a.hubq, a.hub_cnt,
-                                                       a.hub_cap, e->d_ctrl, e->d_hub_id);
+            k_pull<4><<<e->grid_push, BLOCK, 0, st>>>(e->n, e->d_r, e->d_P, e->d_idx, e->d_cache, e->d_ptiles,
+                                                       e->n_ptiles, e->d_ctrl, e->d_hub_id);
         }
         e->launches += 2;
     }
@@ -1598,8 +1607,12 @@ static void enqueue_pass(excent_engine* e, double list_frac, int max_passes, cud
         e->launches++;
     }
     if (pull_edges > 0) {
-        if (e->L == 1) k_pullhub<1><<<e->grid_push, BLOCK, 0, st>>>(e->d_r, e->d_P, a.hubq, a.hub_cnt, a.hub_cap, e->d_ctrl, e->d_hub_id);
-        else k_pullhub<4><<<e->grid_push, BLOCK, 0, st>>>(e->d_r, e->d_P, a.hubq, a.hub_cnt, a.hub_cap, e->d_ctrl, e->d_hub_id);
+        if (e->L == 1)
+            k_pullhub<1><<<e->grid_push, BLOCK, 0, st>>>(e->d_r, e->d_P, e->d_cache, e->d_psegs, e->n_psegs, e->d_ctrl,
+                                                          e->d_hub_id);
+        else
+            k_pullhub<4><<<e->grid_push, BLOCK, 0, st>>>(e->d_r, e->d_P, e->d_cache, e->d_psegs, e->n_psegs, e->d_ctrl,
+                                                          e->d_hub_id);
         e->launches++;
     }
     if (ev) cudaEventRecord(ev[4], st);
@@ -1674,6 +1687,48 @@ extern "C" int excent_engine_seed(excent_engine* e, int k, const int32_t* vids, 
     return EXCENT_OK;
 }
 
+// The static work table of gather passes (from the offsets, once per graph).
+static int build_pull_tables(excent_engine* e) {
+    std::vector<ull> idx((size_t)e->n + 1);
+    EX_CUDA(cudaMemcpy(idx.data(), e->d_idx, idx.size() * sizeof(ull), cudaMemcpyDeviceToHost));
+    std::vector<PullTile> tiles;
+    std::vector<PullSeg> segs;
+    const unsigned ng = (unsigned)(((ull)e->n + 31) / 32);
+    ull acc = 0;
+    unsigned g0 = 0;
+    for (unsigned g = 0; g < ng; g++) {
+        const ull v0 = (ull)g * 32, v1 = std::min<ull>(v0 + 32, (ull)e->n);
+        for (ull v = v0; v < v1; v++) {
+            const ull d = idx[v + 1] - idx[v];
+            if (d > HUB_MIN) {
+                for (ull o = 0; o < d; o += HUB_SEG)
+                    segs.push_back(PullSeg{idx[v] + o, (unsigned)std::min<ull>(HUB_SEG, d - o), (int)v});
+            } else {
+                acc += d;
+            }
+        }
+        acc += 32;   // the group's offsets and bookkeeping
+        if (acc >= PULL_TILE || g + 1 == ng) {
+            tiles.push_back(PullTile{g0, g + 1 - g0});
+            g0 = g + 1;
+            acc = 0;
+        }
+    }
+    invalidate_graph(e);
+    if (e->d_ptiles) cudaFree(e->d_ptiles);
+    if (e->d_psegs) cudaFree(e->d_psegs);
+    e->d_ptiles = nullptr;
+    e->d_psegs = nullptr;
+    EX_ALLOC(e->d_ptiles, std::max<size_t>(tiles.size(), 1) * sizeof(PullTile));
+    EX_ALLOC(e->d_psegs, std::max<size_t>(segs.size(), 1) * sizeof(PullSeg));
+    if (!tiles.empty()) EX_CUDA(cudaMemcpy(e->d_ptiles, tiles.data(), tiles.size() * sizeof(PullTile), cudaMemcpyHostToDevice));
+    if (!segs.empty()) EX_CUDA(cudaMemcpy(e->d_psegs, segs.data(), segs.size() * sizeof(PullSeg), cudaMemcpyHostToDevice));
+    e->n_ptiles = (int)tiles.size();
+    e->n_psegs = (int)segs.size();
+    e->pull_stale = false;
+    return EXCENT_OK;
+}
+
 static int solve_impl(excent_engine* e, double list_frac, int max_passes, int use_graph, bool init) {
     EX_CHECK_ARG(e, "null engine");
     EX_CHECK_ARG(max_passes >= 0 && max_passes < e->log_cap, "max_passes must be < %d", e->log_cap);
@@ -1685,6 +1740,7 @@ static int solve_impl(excent_engine* e, double list_frac, int max_passes, int us
     EX_CUDA(cudaMemcpyAsync(e->d_cmode, cm.data(), e->nc, cudaMemcpyHostToDevice, e->s_main));
     if (init) EX_TRY(init_state(e));
     else EX_TRY(reset_counters(e));
+    if (e->pull_frac > 0 && e->d_P && !e->h_hcache && e->pull_stale) EX_TRY(build_pull_tables(e));
     if (e->hubs_first && e->hubv_stale) {
         // count the high-degree vertices, then list them in a buffer of that size
         if (!e->d_hubv_cnt) EX_ALLOC(e->d_hubv_cnt, sizeof(ull));
