@@ -14,7 +14,7 @@
 // row against eps, takes and pushes the pending lanes and marks every
 // receiving neighbour in the other touched bitmap (check before atomic OR).
 // The solve ends after a pass that pushed nothing. One persistent kernel does
-// the scan, take and push; lists longer than 2048 entries are split into
+// the scan, take and push; lists longer than 512 entries are split into
 // segments handled by a second kernel; a one-thread kernel advances the pass
 // and sets the loop condition of the CUDA graph that runs all passes.
 #include <cuda_runtime.h>
@@ -30,8 +30,8 @@
 namespace excent {
 
 static constexpr int BB = 256;              // threads per block
-static constexpr unsigned BHUB_MIN = 2048;  // lists longer than this go to segments
-static constexpr unsigned BHUB_SEG = 2048;
+static constexpr unsigned BHUB_MIN = 512;   // lists longer than this go to segments
+static constexpr unsigned BHUB_SEG = 512;
 
 struct BSeg {
     const int* nb;
@@ -71,11 +71,6 @@ struct BArgs {
     int greedy;               // take every nonzero lane of a pushed row, not only the pending ones
 };
 
-__device__ __forceinline__ void mark(uint32_t* t, int u) {
-    const uint32_t bit = 1u << (u & 31);
-    if (!(t[u >> 5] & bit)) atomicOr(&t[u >> 5], bit);
-}
-
 __device__ __forceinline__ float take_lane(float* rp, float rv, float eps) {
     return fabsf(rv) > eps ? atomicExch(rp, 0.f) : 0.f;
 }
@@ -87,12 +82,19 @@ __device__ __forceinline__ float take_lane(float* rp, float rv, float eps) {
 __device__ __forceinline__ ull scatter_lanes(const BArgs& a, uint32_t* nxt, const int* nb, unsigned deg,
                                              const float4* gp, const int* gi, int nact, int lane) {
     ull upd = 0;
-    for (unsigned e0 = 0; e0 < deg; e0 += 32) {
-        if (e0 + lane < deg) {
-            const int u = ld_edge(nb + e0 + lane);
-            float4* row = a.R + (size_t)u * a.V;
+    for (unsigned e0 = 0; e0 < deg; e0 += 128) {
+        int u[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {   // four index loads in flight before the reductions
+            const unsigned e = e0 + 32 * k + lane;
+            u[k] = e < deg ? ld_edge(nb + e) : -1;
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (u[k] < 0) continue;
+            float4* row = a.R + (size_t)u[k] * a.V;
             for (int i = 0; i < nact; i++) red_add(row, gi[i], gp[i]);
-            mark(nxt, u);
+            atomicOr(&nxt[u[k] >> 5], 1u << (u[k] & 31));   // result unused: a fire-and-forget reduction
             upd += (ull)nact;
         }
     }
@@ -207,7 +209,7 @@ __global__ void __launch_bounds__(BB) k_bpass(BArgs a) {
             }
             const int* nb = a.adj + b0;
             if (deg > BHUB_MIN) {
-                // queue: weight row into the hub buffer, segments of 2048 entries
+                // queue: weight row into the hub buffer, segments of BHUB_SEG entries
                 ull slot = 0, sbase = 0;
                 const unsigned nseg = (deg + BHUB_SEG - 1) / BHUB_SEG;
                 if (lane == 0) {
@@ -289,6 +291,15 @@ __global__ void __launch_bounds__(BB) k_bhub(BArgs a) {
         for (int i = 0; i < BB / 32; i++) tu += s_u[i];
         if (tu) atomicAdd(&a.ctrl->total_lane_e, tu);
     }
+}
+
+// Vertices with more than thr entries.
+__global__ void k_bcount(int n, const ull* idx, unsigned thr, ull* out) {
+    ull c = 0;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x)
+        c += idx[v + 1] - idx[v] > thr;
+    c = warp_sum(c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
 }
 
 // End of a pass: totals, next pass's counters, loop condition.
@@ -418,7 +429,18 @@ static int batch_setup(excent_batch* b, int device, int n, ull m, const ull* d_i
     const size_t words = ((size_t)n + 31) / 32;
     BX_ALLOC(b->d_t[0], words * 4);
     BX_ALLOC(b->d_t[1], words * 4);
-    b->prow_cap = m / BHUB_MIN + 16;
+    {   // rows that can be queued in one pass: the vertices with more than BHUB_MIN entries
+        ull* d_cnt = nullptr;
+        BX_ALLOC(d_cnt, sizeof(ull));
+        cudaMemset(d_cnt, 0, sizeof(ull));
+        k_bcount<<<b->sms * 8, BB, 0, b->st>>>(n, d_idx, BHUB_MIN, d_cnt);
+        ull cnt = 0;
+        const cudaError_t err = cudaMemcpyAsync(&cnt, d_cnt, sizeof(ull), cudaMemcpyDeviceToHost, b->st);
+        cudaStreamSynchronize(b->st);
+        cudaFree(d_cnt);
+        EX_CUDA(err);
+        b->prow_cap = cnt + 16;
+    }
     b->seg_cap = 2 * (m / BHUB_SEG) + 64;
     BX_ALLOC(b->d_P, b->prow_cap * (size_t)B * sizeof(float));
     BX_ALLOC(b->d_seg, b->seg_cap * sizeof(BSeg));

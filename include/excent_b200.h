@@ -371,7 +371,7 @@ int excent_batch_seed(excent_batch* b, int nq, const int* lane_off, const int32_
 int excent_batch_solve(excent_batch* b, int max_passes, int use_graph);
 /* Passes, pushed vertices, pushed adjacency entries, 16-byte lane-group
  * reductions issued, touched rows examined and segments of lists longer than
- * 2048 entries queued by the last solve (any output may be NULL). */
+ * 512 entries queued by the last solve (any output may be NULL). */
 int excent_batch_stats(excent_batch* b, int* passes, unsigned long long* pushed_vertices,
                        unsigned long long* pushed_edges, unsigned long long* lane_updates,
                        unsigned long long* rows_checked, unsigned long long* hub_segments);
