@@ -81,6 +81,8 @@ def parse():
     ap.add_argument("--ooc-mode", default="pinned", choices=["pinned", "pipeline"],
                     help="which of this repo's out-of-core arms is the headline")
     ap.add_argument("--ooc-ref", default="on", choices=["on", "off"], help="also run the reference CLI out of core")
+    ap.add_argument("--list-frac", type=float, default=0.5,
+                    help="per-chunk list/range rule of the device loop (the reference's --list-frac)")
     ap.add_argument("--log-dir", default=None, help="keep the stdout of every CLI run in this directory")
     ap.add_argument("--hub-first", default="on", choices=["on", "off"],
                     help="push the high-degree lists first in every pass")
@@ -198,7 +200,7 @@ def run_ours(a, world, rank, local, dist):
     eng.set_hub_order(a.hub_first == "on")
     use_graph = not a.no_graph
     for _ in range(a.warmup):
-        s = eng.solve(use_graph=use_graph)
+        s = eng.solve(list_frac=a.list_frac, use_graph=use_graph)
         log(f"warmup solve: {s.passes} passes, {s.pushed} entries pushed")
     st = torch.cuda.ExternalStream(eng.stream())
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -212,7 +214,7 @@ def run_ours(a, world, rank, local, dist):
     pushed = 0
     passes = []
     for _ in range(a.steps):
-        s = eng.solve(use_graph=use_graph)
+        s = eng.solve(list_frac=a.list_frac, use_graph=use_graph)
         pushed += s.pushed
         passes.append(s.passes)
     ev1.record(st)
@@ -240,7 +242,7 @@ def run_ours(a, world, rank, local, dist):
     for _ in range(a.steps):
         eng.upload_offsets(h_idx.data_ptr())
         eng.load_cache(0, m, h_adj.data_ptr())
-        s = eng.solve(use_graph=use_graph)
+        s = eng.solve(list_frac=a.list_frac, use_graph=use_graph)
         e_pushed += s.pushed
         for i in range(nm):
             eng.read(i, out=outs[i])
@@ -254,7 +256,7 @@ def run_ours(a, world, rank, local, dist):
     log(f"e2e: {a.steps} solves in {te:.3f}s")
     # roofline of the dominant kernel (push + its hub tail), per-kernel events on a profiled solve
     eng.profile(True)
-    eng.solve(use_graph=False)
+    eng.solve(list_frac=a.list_frac, use_graph=False)
     s, plog = eng.stats(with_log=True)
     prof, ppasses = eng.profile_read()
     eng.profile(False)
@@ -284,7 +286,7 @@ def run_ours(a, world, rank, local, dist):
                    "l2_note": "inputs larger than L2 (edge cache %.2f GB)" % (m * 4 / 1e9),
                    "cuda_graph": use_graph, "parallelism": f"{world} independent replicas",
                    "ev_init": a.ev_init, "ev_project": a.ev_project if measure == "all" else None,
-                   "pull_frac": a.pull_frac, "hub_targets": hub_k,
+                   "pull_frac": a.pull_frac, "hub_targets": hub_k, "list_frac": a.list_frac,
                    "hub_first": a.hub_first},
         "e2e": {"value": round(e_pushed / te / 1e9, 4), "unit": "GTEPS", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": round(te / a.steps * 1e3, 3),
@@ -671,7 +673,8 @@ def run_ooc(a, world, rank, local, dist):
             if measure in ("ev", "all", "katz"):
                 return {"metric": "GTEPS (out of core)", "unavailable": "eigenvector/Katz constants need the "
                         "FP64 lambda1 of the full graph, not computed out of core here"}
-            arms = [("ours_pinned", K.CLI_PATH, ["--host-cache", "pinned"]), ("ours", K.CLI_PATH, [])]
+            arms = [("ours_pinned", K.CLI_PATH, ["--host-cache", "pinned", "--list-frac", str(a.list_frac)]),
+                    ("ours", K.CLI_PATH, [])]
             if a.ooc_ref == "on" and os.path.exists(ref_bin):
                 arms.append(("reference", ref_bin, []))
             for name, binary, extra in arms:
