@@ -94,7 +94,8 @@ __device__ __forceinline__ ull scatter_lanes(const BArgs& a, uint32_t* nxt, cons
             if (u[k] < 0) continue;
             float4* row = a.R + (size_t)u[k] * a.V;
             for (int i = 0; i < nact; i++) red_add(row, gi[i], gp[i]);
-            atomicOr(&nxt[u[k] >> 5], 1u << (u[k] & 31));   // result unused: a fire-and-forget reduction
+            const uint32_t bit = 1u << (u[k] & 31);   // check first: most targets are marked already
+            if (!(nxt[u[k] >> 5] & bit)) atomicOr(&nxt[u[k] >> 5], bit);
             upd += (ull)nact;
         }
     }

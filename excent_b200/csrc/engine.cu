@@ -342,7 +342,11 @@ __global__ void k_plan(int nc, const int* cv0, int n, ull* cnt, const uint8_t* c
         uint8_t ty = WT_NONE;
         if (!stop && !pull && c < nc && cmode[c] && cnt[2 * c] > 0) {
             const int v0 = cv0[c], v1 = c + 1 < nc ? cv0[c + 1] : n;
-            if ((double)cnt[2 * c] < list_frac * (v1 - v0)) { ty = WT_LIST; items = (unsigned)cnt[2 * c]; atomicAdd(&s_nl, 1); }
+            // chunks read from host memory (mode 2) always push as ranges: a vertex that turns
+            // pending during the pass is pushed in it, which saves whole passes over the link
+            if (cmode[c] != 2 && (double)cnt[2 * c] < list_frac * (v1 - v0)) {
+                ty = WT_LIST; items = (unsigned)cnt[2 * c]; atomicAdd(&s_nl, 1);
+            }
             else { ty = WT_RANGE; items = (unsigned)(v1 - v0); atomicAdd(&s_nr, 1); }
         }
         s_scan[t] = items;
@@ -1737,7 +1741,9 @@ static int solve_impl(excent_engine* e, double list_frac, int max_passes, int us
                      "chunk %d is neither in the edge cache nor in the host cache", c);
     EX_CUDA(cudaSetDevice(e->dev));
     std::vector<uint8_t> cm(e->nc, 1);
-    EX_CUDA(cudaMemcpyAsync(e->d_cmode, cm.data(), e->nc, cudaMemcpyHostToDevice, e->s_main));
+    for (int c = 0; c < e->nc; c++)
+        if (e->h_hcache && e->ce[c] >= e->cache_edges) cm[c] = 2;   // lists in host memory
+    EX_CUDA(cudaMemcpy(e->d_cmode, cm.data(), e->nc, cudaMemcpyHostToDevice));
     if (init) EX_TRY(init_state(e));
     else EX_TRY(reset_counters(e));
     if (e->pull_frac > 0 && e->d_P && !e->h_hcache && e->pull_stale) EX_TRY(build_pull_tables(e));
