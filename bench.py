@@ -81,6 +81,9 @@ def parse():
     ap.add_argument("--ooc-mode", default="pinned", choices=["pinned", "pipeline"],
                     help="which of this repo's out-of-core arms is the headline")
     ap.add_argument("--ooc-ref", default="on", choices=["on", "off"], help="also run the reference CLI out of core")
+    ap.add_argument("--batch-width", type=int, default=0, choices=[0, 32, 64, 128, 256],
+                    help="batched PPR: fixed batch width instead of the autotuner's")
+    ap.add_argument("--greedy", default="off", choices=["on", "off"], help="with --batch-width: greedy row push")
     ap.add_argument("--list-frac", type=float, default=0.5,
                     help="per-chunk list/range rule of the device loop (the reference's --list-frac)")
     ap.add_argument("--log-dir", default=None, help="keep the stdout of every CLI run in this directory")
@@ -337,14 +340,18 @@ def run_ppr(a, world, rank, local, dist):
     vals = [(1 - d) / len(q) for q in qs]
     eps = 1e-4 * (1 - d)
     log(f"graph scale {scale}: n={n} m={m}; {len(qs)} queries on this rank")
-    best, greedy, table = X.autotune_batch(n, m, di, da, qs, vals, eps, "ppr", d, device=local)
+    if a.batch_width:
+        best, greedy, table = a.batch_width, a.greedy == "on", {}
+    else:
+        best, greedy, table = X.autotune_batch(n, m, di, da, qs, vals, eps, "ppr", d, device=local)
     log(f"autotune: per-query ms {table} -> B={best} greedy={greedy}")
+    use_graph = not a.no_graph
     b = X.Batch(n, m, di, da, best, "ppr", d, device=local)
     b.set_greedy(greedy)
     st = torch.cuda.ExternalStream(b.stream())
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     b.seed(qs[:best], vals[:best], eps)   # warm-up (graph build)
-    b.solve()
+    b.solve(use_graph=use_graph)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -354,7 +361,7 @@ def run_ppr(a, world, rank, local, dist):
     counters = {"pushed_vertices": 0, "lane_updates": 0, "rows_checked": 0, "hub_segments": 0}
     for i in range(0, len(qs), best):
         b.seed(qs[i:i + best], vals[i:i + best], eps)
-        s = b.solve()
+        s = b.solve(use_graph=use_graph)
         tot_e += s["pushed_edges"]
         passes.append(s["passes"])
         for k in counters:
@@ -363,7 +370,7 @@ def run_ppr(a, world, rank, local, dist):
     torch.cuda.synchronize()
     t_batch = ev0.elapsed_time(ev1) / 1e3
     b.seed(qs[:best], vals[:best], eps)   # first batch again, for the comparison below (untimed)
-    b.solve()
+    b.solve(use_graph=use_graph)
     xb = [b.read(j) for j in range(min(4, len(qs)))]
     log(f"batched: {len(qs)} queries in {t_batch:.3f}s, passes {passes}")
     # the same queries one at a time through the plain engine (seeded PageRank, full snapshot per pass)
@@ -374,7 +381,7 @@ def run_ppr(a, world, rank, local, dist):
     eng = X.Engine(n, m, meas, v0, e, device=local)
     eng.upload_device(di, da)
     X.seed_engine(eng, qs[0], vals[0])
-    X.resume(eng)
+    X.resume(eng, use_graph=use_graph)
     se = torch.cuda.ExternalStream(eng.stream())
     torch.cuda.synchronize()
     ev0.record(se)
@@ -382,7 +389,7 @@ def run_ppr(a, world, rank, local, dist):
     xs = []
     for j, q in enumerate(qs):
         X.seed_engine(eng, q, vals[j])
-        s = X.resume(eng)
+        s = X.resume(eng, use_graph=use_graph)
         seq_e += s.pushed
         if j < 4:
             xs.append(eng.read(0))
