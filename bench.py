@@ -663,6 +663,24 @@ def run_ooc(a, world, rank, local, dist):
         torch.cuda.synchronize()
         link = h2d_gbs(torch)
         log(f"pinned H2D {link:.1f} GB/s")
+        lam = None
+        if "ev" in a.ooc_measures.split(","):
+            # lambda1 in FP64 with the whole graph on the device (it fits in HBM; the solve is then
+            # run with the device memory held to the budget)
+            mm = np.memmap(path, dtype=np.uint8, mode="r")
+            off_idx, off_adj = 16, 16 + 8 * (n + 1)
+            d_idx = torch.from_numpy(np.frombuffer(mm[off_idx:off_adj], dtype=np.int64).copy()).cuda()
+            d_adj = torch.empty(m, dtype=torch.int32, device="cuda")
+            step = 1 << 28
+            for e0 in range(0, m, step):
+                e1 = min(m, e0 + step)
+                d_adj[e0:e1].copy_(torch.from_numpy(
+                    np.frombuffer(mm[off_adj + 4 * e0:off_adj + 4 * e1], dtype=np.int32).copy()))
+            par = X.params_fp64(n, d_idx.data_ptr(), d_adj.data_ptr(), device=local)
+            lam = par["lambda"]
+            log(f"lambda1 {lam:.6f} after {par['sweeps']} FP64 sweeps")
+            del d_idx, d_adj, mm
+            torch.cuda.empty_cache()
         free, total = torch.cuda.mem_get_info()
         keep = int(a.ooc_budget_gb * 1e9)
         ballast = None
@@ -677,9 +695,10 @@ def run_ooc(a, world, rank, local, dist):
         runs = {}
         for measure in a.ooc_measures.split(","):
             args = [path, "--measure", measure, "--count-pushes"]
-            if measure in ("ev", "all", "katz"):
-                return {"metric": "GTEPS (out of core)", "unavailable": "eigenvector/Katz constants need the "
-                        "FP64 lambda1 of the full graph, not computed out of core here"}
+            if measure == "ev":
+                args += ["--lambda", "%.17g" % lam, "--eps-ev", "1e-6", "--max-passes", str(a.ref_passes)]
+            elif measure != "pr":
+                return {"metric": "GTEPS (out of core)", "unavailable": f"measure {measure} is not part of this run"}
             arms = [("ours_pinned", K.CLI_PATH, ["--host-cache", "pinned", "--list-frac", str(a.list_frac)]),
                     ("ours", K.CLI_PATH, [])]
             if a.ooc_ref == "on" and os.path.exists(ref_bin):
@@ -715,6 +734,7 @@ def run_ooc(a, world, rank, local, dist):
             "ms_per_step": round(ours["passes_s"] * 1e3, 1), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded R-MAT written as EGR on local disk)",
             "config": {"workload": f"{a.ooc_measures} out of core on R-MAT scale {scale} EF {ef} seed {seed}",
+                       "lambda1": lam, "ev_max_passes": a.ref_passes if lam else None,
                        "headline_arm": head + (" (--host-cache pinned: lists read in place from pinned host memory)"
                                                if head == "ours_pinned" else " (host gather/stream pipeline)"),
                        "n": n, "m": m, "egr_gb": round(os.path.getsize(path) / 1e9, 2), "partitions": parts,
