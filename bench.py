@@ -87,8 +87,8 @@ def parse():
     ap.add_argument("--list-frac", type=float, default=0.5,
                     help="per-chunk list/range rule of the device loop (the reference's --list-frac)")
     ap.add_argument("--log-dir", default=None, help="keep the stdout of every CLI run in this directory")
-    ap.add_argument("--hub-first", default="on", choices=["on", "off"],
-                    help="push the high-degree lists first in every pass")
+    ap.add_argument("--hub-order", default="first", choices=["first", "last", "table"],
+                    help="where the high-degree lists go in each pass of the device loop")
     ap.add_argument("--hub-targets", type=int, default=-1,
                     help="shared-memory aggregation of the k highest-degree targets (0: off; -1: 8192 for "
                          "one measure, 2048 for all)")
@@ -200,7 +200,7 @@ def run_ours(a, world, rank, local, dist):
     eng.set_pull(a.pull_frac)
     hub_k = a.hub_targets if a.hub_targets >= 0 else min(8192 if nm == 1 else 2048, n)
     eng.set_hub_targets(hub_k)
-    eng.set_hub_order(a.hub_first == "on")
+    eng.set_hub_order(a.hub_order)
     use_graph = not a.no_graph
     for _ in range(a.warmup):
         s = eng.solve(list_frac=a.list_frac, use_graph=use_graph)
@@ -290,7 +290,7 @@ def run_ours(a, world, rank, local, dist):
                    "cuda_graph": use_graph, "parallelism": f"{world} independent replicas",
                    "ev_init": a.ev_init, "ev_project": a.ev_project if measure == "all" else None,
                    "pull_frac": a.pull_frac, "hub_targets": hub_k, "list_frac": a.list_frac,
-                   "hub_first": a.hub_first},
+                   "hub_order": a.hub_order},
         "e2e": {"value": round(e_pushed / te / 1e9, 4), "unit": "GTEPS", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": round(te / a.steps * 1e3, 3),
                 "wall_ms_per_step": round(te_wall / a.steps * 1e3, 3)},
@@ -699,7 +699,8 @@ def run_ooc(a, world, rank, local, dist):
                 args += ["--lambda", "%.17g" % lam, "--eps-ev", "1e-6", "--max-passes", str(a.ref_passes)]
             elif measure != "pr":
                 return {"metric": "GTEPS (out of core)", "unavailable": f"measure {measure} is not part of this run"}
-            arms = [("ours_pinned", K.CLI_PATH, ["--host-cache", "pinned", "--list-frac", str(a.list_frac)]),
+            arms = [("ours_pinned", K.CLI_PATH, ["--host-cache", "pinned", "--list-frac", str(a.list_frac),
+                                                 "--hub-order", a.hub_order]),
                     ("ours", K.CLI_PATH, [])]
             if a.ooc_ref == "on" and os.path.exists(ref_bin):
                 arms.append(("reference", ref_bin, []))

@@ -206,9 +206,11 @@ class Engine:
         """Shared-memory aggregation of the contributions to the k highest-degree targets (0: off)."""
         call("excent_engine_set_hub_targets", self.h, int(k))
 
-    def set_hub_order(self, first=True):
-        """Device solve: push the lists longer than 256 entries first in every pass."""
-        call("excent_engine_set_hub_order", self.h, int(bool(first)))
+    def set_hub_order(self, order="first"):
+        """Device solve: where the lists longer than 256 entries go in each pass
+        ("first", "last", or "table": with the rest)."""
+        code = {"table": 0, "first": 1, "last": 2, False: 0, True: 1}[order]
+        call("excent_engine_set_hub_order", self.h, code)
 
     def host_cache(self):
         """Pinned host memory for the entries past the edge cache (excent_engine_host_cache):

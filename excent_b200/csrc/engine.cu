@@ -117,7 +117,7 @@ struct PushArgs {
     // (hubv[*hubv_cnt]) first; SRC_TABLE then skips them
     const int* hubv;
     const ull* hubv_cnt;
-    int hubs_first;
+    int skip_hubs;      // SRC_TABLE leaves the lists longer than HUB_MIN to SRC_HUBS
     // lists past the device cache read in place from pinned host memory (zero copy)
     const int* hcache;   // entries [cache_edges, m), device-mapped
     ull cache_edges;
@@ -481,7 +481,7 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
         T p{};
         bool act = false;
         if (get_item<SRC>(a, tile * 32 + lane, v, nb, deg) &&
-            !(SRC == SRC_TABLE && a.hubs_first && deg > HUB_MIN)) {   // pushed first by SRC_HUBS
+            !(SRC == SRC_TABLE && a.skip_hubs && deg > HUB_MIN)) {   // pushed by SRC_HUBS
             p = take(x, r, v, deg, a.M);
             act = nonzero(p) && deg > 0;
         }
@@ -931,7 +931,7 @@ struct excent_engine {
     int* d_hubv = nullptr;   // high-degree-first order: vertices with lists longer than HUB_MIN
     ull* d_hubv_cnt = nullptr;
     ull hubv_cap = 0;
-    bool hubs_first = true;
+    int hub_order = 1;       // high-degree lists: 0 in table order, 1 first, 2 last
     bool hubv_stale = true;
     double pull_frac = 0;    // pull when the pending demand >= pull_frac * m (0: never)
     bool ev_proj = false;
@@ -1335,7 +1335,7 @@ static PushArgs push_args(excent_engine* e, int q) {
     a.hids = e->d_hids; a.hoff = e->d_hoff; a.hedges = e->d_hedges; a.hlist = e->d_hlist;
     a.hubq = e->d_hubq[q]; a.hub_cap = e->hub_cap[q]; a.hub_cnt = e->d_hubcnt + q; a.ctrl = e->d_ctrl;
     a.hub_id = e->d_hub_id; a.hub_k = e->hub_k;
-    a.hubv = e->d_hubv; a.hubv_cnt = e->d_hubv_cnt; a.hubs_first = 0;
+    a.hubv = e->d_hubv; a.hubv_cnt = e->d_hubv_cnt; a.skip_hubs = 0;
     a.hcache = nullptr; a.cache_edges = e->cache_edges;
     if (e->h_hcache) cudaHostGetDevicePointer((void**)&a.hcache, e->h_hcache, 0);
     return a;
@@ -1577,18 +1577,19 @@ static void enqueue_pass(excent_engine* e, double list_frac, int max_passes, cud
     if (ev) cudaEventRecord(ev[2], st);
     PushArgs a = push_args(e, 0);
     const int gt = e->sms * 8;
-    const bool hubs_first = e->hubs_first && e->d_hubv && !e->hubv_stale;
-    if (hubs_first) {
-        // the high-degree lists first, so their (large) share of the pass's residual reaches
-        // every other vertex before that vertex is taken
+    // high-degree order: 1 = the lists longer than HUB_MIN first, so their (large) share of the
+    // pass's residual reaches every other vertex before that vertex is taken; 2 = last, so they
+    // collect the pass's residual and push it once; 0 = in table order with the rest
+    const int order = e->hub_order && e->d_hubv && !e->hubv_stale ? e->hub_order : 0;
+    auto hub_phase = [&]() {
         if (e->L == 1) k_push<1, SRC_HUBS><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
         else k_push<4, SRC_HUBS><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
         if (e->L == 1) k_hub<1><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
         else k_hub<4><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
-        cudaMemsetAsync(a.hub_cnt, 0, sizeof(ull), st);   // the queue is empty again for gather passes
         e->launches += 2;
-        a.hubs_first = 1;
-    }
+    };
+    if (order == 1) hub_phase();
+    a.skip_hubs = order != 0;   // the table push skips the high-degree vertices
     if (e->L == 1) k_push<1, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
     else k_push<4, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
     e->launches++;
@@ -1605,11 +1606,12 @@ static void enqueue_pass(excent_engine* e, double list_frac, int max_passes, cud
         e->launches += 2;
     }
     if (ev) cudaEventRecord(ev[3], st);
-    if (!hubs_first) {   // with the high-degree lists first, the table push queues no segments
+    if (order == 0) {   // the table push's own segments (with a high-degree order it queues none)
         if (e->L == 1) k_hub<1><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
         else k_hub<4><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
         e->launches++;
     }
+    if (order == 2) hub_phase();
     if (pull_edges > 0) {
         if (e->L == 1)
             k_pullhub<1><<<e->grid_push, BLOCK, 0, st>>>(e->d_r, e->d_P, e->d_cache, e->d_psegs, e->n_psegs, e->d_ctrl,
@@ -1747,7 +1749,7 @@ static int solve_impl(excent_engine* e, double list_frac, int max_passes, int us
     if (init) EX_TRY(init_state(e));
     else EX_TRY(reset_counters(e));
     if (e->pull_frac > 0 && e->d_P && !e->h_hcache && e->pull_stale) EX_TRY(build_pull_tables(e));
-    if (e->hubs_first && e->hubv_stale) {
+    if (e->hub_order && e->hubv_stale) {
         // count the high-degree vertices, then list them in a buffer of that size
         if (!e->d_hubv_cnt) EX_ALLOC(e->d_hubv_cnt, sizeof(ull));
         EX_CUDA(cudaMemsetAsync(e->d_hubv_cnt, 0, sizeof(ull), e->s_main));
@@ -1780,7 +1782,7 @@ static int solve_impl(excent_engine* e, double list_frac, int max_passes, int us
         EX_CUDA(cudaGraphLaunch(e->gexec, e->s_main));
         EX_CUDA(cudaStreamSynchronize(e->s_main));
         EX_CUDA(cudaMemcpy(e->h_ctrl, e->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
-        e->launches += ((e->pull_frac > 0 && e->d_P ? 7ull : 4ull) + (e->hubs_first && e->d_hubv ? 1ull : 0ull)) *
+        e->launches += ((e->pull_frac > 0 && e->d_P ? 7ull : 4ull) + (e->hub_order && e->d_hubv ? 1ull : 0ull)) *
                        (e->h_ctrl->pass + 1);
     } else {
         for (int p = 0; p <= max_passes; p++) {
@@ -1935,11 +1937,11 @@ extern "C" int excent_engine_set_hub_targets(excent_engine* e, int k) {
     return EXCENT_OK;
 }
 
-extern "C" int excent_engine_set_hub_order(excent_engine* e, int first) {
-    EX_CHECK_ARG(e, "null engine");
+extern "C" int excent_engine_set_hub_order(excent_engine* e, int order) {
+    EX_CHECK_ARG(e && order >= 0 && order <= 2, "hub order must be 0 (table order), 1 (first) or 2 (last)");
     EX_CUDA(cudaSetDevice(e->dev));
     invalidate_graph(e);
-    e->hubs_first = first != 0;
+    e->hub_order = order;
     return EXCENT_OK;
 }
 

@@ -43,7 +43,7 @@ struct Options {
     bool device_loop = false;  // fully cached graphs: load at setup, run the on-device pass loop
     bool ev_init_fp64 = false; // eigenvector initial residual from the FP64 lambda1
     int hub_targets = -1;      // shared-memory aggregation of the top-degree targets (-1: auto)
-    bool hub_first = true;     // device loop: push the high-degree lists first in every pass
+    int hub_order = 1;         // device loop: the high-degree lists 0 in table order, 1 first, 2 last
     std::string host_cache = "off";   // pinned: entries past the HBM cache read in place from pinned host memory
 };
 
@@ -115,16 +115,12 @@ static int parse_options(int argc, char** argv, Options& o) {
                 o.host_cache = v;
             }
         }
-        else if (a == "--hub-first") {
+        else if (a == "--hub-order") {
             if ((ok = next(v))) {
-                if (strcmp(v, "on") && strcmp(v, "off")) { fprintf(stderr, "--hub-first must be on or off\n"); return 1; }
-                o.hub_first = !strcmp(v, "on");
-            }
-        }
-        else if (a == "--ev-init") {
-            if ((ok = next(v))) {
-                if (strcmp(v, "fp64") && strcmp(v, "reference")) { fprintf(stderr, "--ev-init must be fp64 or reference\n"); return 1; }
-                o.ev_init_fp64 = !strcmp(v, "fp64");
+                if (!strcmp(v, "table")) o.hub_order = 0;
+                else if (!strcmp(v, "first")) o.hub_order = 1;
+                else if (!strcmp(v, "last")) o.hub_order = 2;
+                else { fprintf(stderr, "--hub-order must be first, last or table\n"); return 1; }
             }
         }
         else { fprintf(stderr, "unknown option %s\n", a.c_str()); return 1; }
@@ -246,7 +242,7 @@ static int run(const Options& o) {
                 fprintf(stderr, "excent: hub targets off (%s)\n", excent_last_error());
         }
     }
-    RT_CK(excent_engine_set_hub_order(e, o.hub_first ? 1 : 0));
+    RT_CK(excent_engine_set_hub_order(e, o.hub_order));
     int nh = 0;
     ull hot_edges = 0, hot_deg_min = 0;
     bool hot_mode = hot_mode_req;

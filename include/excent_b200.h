@@ -226,12 +226,13 @@ int excent_engine_read_trace(excent_engine* e, uint16_t* out);
  * turns it off. No reference counterpart. */
 int excent_engine_set_hub_targets(excent_engine* e, int k);
 
-/* High-degree-first order for the device solve: each pass pushes the lists
- * longer than 256 entries first (and their segments), then every other
- * pending vertex, so the large share of a pass's residual carried by the
- * high-degree vertices reaches the others before they are taken. On by
- * default. No reference counterpart (the reference pushes chunk by chunk). */
-int excent_engine_set_hub_order(excent_engine* e, int first);
+/* Order of the high-degree lists (more than 256 entries) in each pass of the
+ * device solve: 1 (default) first, so the large share of a pass's residual they
+ * carry reaches the other vertices before those are taken; 2 last, after every
+ * other pending vertex, so they collect the pass's residual and push it once;
+ * 0 in table order with the rest. No reference counterpart (the reference
+ * pushes chunk by chunk, its degree cache at the end of a pass by default). */
+int excent_engine_set_hub_order(excent_engine* e, int order);
 
 /* Host cache for graphs larger than device memory: pinned, device-mapped host
  * memory for the entries past the HBM edge cache (entries [*first_edge, m),

@@ -399,11 +399,11 @@ def test_high_degree_first_order(rmat16, measure, use_graph, pull):
     names = ["pr", "katz", "ev"] if measure == "all" else ["pr"]
     assert int((np.diff(idx) > 256).sum()) > 0
     res = {}
-    for mode in ("plain", "first", "first+targets"):
+    for mode in ("plain", "first", "last", "first+targets"):
         meas = X.measures(measure, **kw)
         eng = make_engine(n, idx, adj, meas)
         eng.set_pull(pull)
-        eng.set_hub_order(mode != "plain")
+        eng.set_hub_order({"plain": "table", "first": "first", "last": "last", "first+targets": "first"}[mode])
         if mode == "first+targets":
             eng.set_hub_targets(512)
             eng.load_cache(0, len(adj), np.ascontiguousarray(adj, dtype=np.int32))
@@ -416,7 +416,7 @@ def test_high_degree_first_order(rmat16, measure, use_graph, pull):
         res[(mode, "pushed")] = st.pushed
         eng.close()
     print(res)
-    for mode in ("first", "first+targets"):
+    for mode in ("first", "last", "first+targets"):
         for name in names:
             assert res[(mode, name)]["l1_rel"] <= 1.25 * res[("plain", name)]["l1_rel"] + 1e-5, (mode, name, res)
 
