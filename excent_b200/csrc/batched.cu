@@ -79,7 +79,7 @@ __device__ __forceinline__ float take_lane(float* rp, float rv, float eps) {
 // takes entry e0 + i and adds the row's nact active 16-byte groups (indices
 // gi[], weights gp[] in shared memory, the same for every lane) to that
 // target's row, so a warp keeps 32 targets in flight.
-__device__ __forceinline__ ull scatter_lanes(const BArgs& a, uint32_t* nxt, const int* nb, unsigned deg,
+__device__ __forceinline__ ull scatter_lanes(float4* R, int V, uint32_t* nxt, const int* nb, unsigned deg,
                                              const float4* gp, const int* gi, int nact, int lane) {
     ull upd = 0;
     for (unsigned e0 = 0; e0 < deg; e0 += 128) {
@@ -92,7 +92,7 @@ __device__ __forceinline__ ull scatter_lanes(const BArgs& a, uint32_t* nxt, cons
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             if (u[k] < 0) continue;
-            float4* row = a.R + (size_t)u[k] * a.V;
+            float4* row = R + (size_t)u[k] * V;
             for (int i = 0; i < nact; i++) red_add(row, gi[i], gp[i]);
             const uint32_t bit = 1u << (u[k] & 31);   // check first: most targets are marked already
             if (!(nxt[u[k] >> 5] & bit)) atomicOr(&nxt[u[k] >> 5], bit);
@@ -126,7 +126,7 @@ __device__ __forceinline__ int compact_groups(const float4 (&p)[NV], const bool 
 
 // One pass: scan touched words (interleaved over warps), check, take and push.
 template <int LPR, int NV>
-__global__ void __launch_bounds__(BB) k_bpass(BArgs a) {
+__global__ void __launch_bounds__(BB, 4) k_bpass(BArgs a) {
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int j0 = lane % LPR;
     const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(BB) k_bpass(BArgs a) {
                 continue;
             }
             const int nact = compact_groups<LPR, NV>(p, act, s_gp[wib], s_gi[wib], lane);
-            upd += scatter_lanes(a, nxt, nb, deg, s_gp[wib], s_gi[wib], nact, lane);
+            upd += scatter_lanes(a.R, a.V, nxt, nb, deg, s_gp[wib], s_gi[wib], nact, lane);
             __syncwarp();
         }
     }
@@ -280,7 +280,7 @@ __global__ void __launch_bounds__(BB) k_bhub(BArgs a) {
             act[k] = nonzero(p[k]);
         }
         const int nact = compact_groups<LPR, NV>(p, act, s_gp[wib], s_gi[wib], lane);
-        upd += scatter_lanes(a, nxt, sg.nb, sg.len, s_gp[wib], s_gi[wib], nact, lane);
+        upd += scatter_lanes(a.R, a.V, nxt, sg.nb, sg.len, s_gp[wib], s_gi[wib], nact, lane);
         __syncwarp();
     }
     __shared__ ull s_u[BB / 32];
