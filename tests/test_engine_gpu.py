@@ -418,7 +418,8 @@ def test_high_degree_first_order(rmat16, measure, use_graph, pull):
     print(res)
     for mode in ("first", "last", "first+targets"):
         for name in names:
-            assert res[(mode, name)]["l1_rel"] <= 1.25 * res[("plain", name)]["l1_rel"] + 1e-5, (mode, name, res)
+            # eps-level slack: the eps of Katz and EV here is 1e-5
+            assert res[(mode, name)]["l1_rel"] <= 1.25 * res[("plain", name)]["l1_rel"] + 3e-5, (mode, name, res)
 
 
 @pytest.mark.parametrize("measure", ["pr", "all"])
