@@ -102,6 +102,39 @@ __device__ __forceinline__ ull scatter_lanes(float4* R, int V, uint32_t* nxt, co
     return upd;
 }
 
+// Scatter for rows with many active groups: the lanes over the row's groups
+// (lane j0 + LPR * k of each LPR-lane sub-warp), 32 / LPR target rows per
+// step, so each reduction instruction covers one contiguous stretch of a
+// target row instead of 32 unrelated rows.
+template <int LPR, int NV>
+__device__ __forceinline__ ull scatter_rowpar(float4* R, int V, uint32_t* nxt, const int* nb, unsigned deg,
+                                              const float4 (&p)[NV], const bool (&act)[NV], int lane) {
+    constexpr int RPW = 32 / LPR;
+    const int sub = lane / LPR, j0 = lane % LPR;
+    ull upd = 0;
+    for (unsigned e0 = 0; e0 < deg; e0 += 32) {
+        const int ul = e0 + lane < deg ? ld_edge(nb + e0 + lane) : -1;
+        const unsigned cnt = min(32u, deg - e0);
+        for (unsigned g = 0; g < cnt; g += RPW) {
+            const int u = __shfl_sync(FULL, ul, (int)g + sub);
+            if (g + sub < cnt) {
+                float4* row = R + (size_t)u * V;
+#pragma unroll
+                for (int k = 0; k < NV; k++)
+                    if (act[k]) { red_add(row, j0 + LPR * k, p[k]); upd++; }
+                if (j0 == 0) {
+                    const uint32_t bit = 1u << (u & 31);
+                    if (!(nxt[u >> 5] & bit)) atomicOr(&nxt[u >> 5], bit);
+                }
+            }
+        }
+    }
+    return upd;
+}
+
+// Rows with more active 16-byte groups than this scatter over their groups.
+static constexpr int DENSE_GROUPS = 16;
+
 // Compact the active groups of a row held by lanes j0 + LPR * k (k < NV) into
 // the warp's shared lists; returns their count (warp-uniform).
 template <int LPR, int NV>
@@ -140,11 +173,17 @@ __global__ void __launch_bounds__(BB, 4) k_bpass(BArgs a) {
     float4 eps[NV];
 #pragma unroll
     for (int k = 0; k < NV; k++) eps[k] = a.eps[j0 + LPR * k];
-    for (long long w = gw; w < a.words; w += nwarps) {
-        uint32_t bits = cur[w];
-        if (!bits) continue;
-        __syncwarp();
-        if (lane == 0) { cur[w] = 0; checked += __popc(bits); }
+    for (long long w0 = gw * 32; w0 < a.words; w0 += nwarps * 32) {
+        // 32 words per step, one per lane; then the warp walks the nonzero ones
+        const long long wl = w0 + lane;
+        const uint32_t mine = wl < a.words ? cur[wl] : 0u;
+        if (mine) { cur[wl] = 0; checked += __popc(mine); }
+        unsigned nzw = __ballot_sync(FULL, mine != 0);
+        while (nzw) {
+        const int src = __ffs(nzw) - 1;
+        nzw &= nzw - 1;
+        const long long w = w0 + src;
+        uint32_t bits = __shfl_sync(FULL, mine, src);
         while (bits) {
             const int b = __ffs(bits) - 1;
             bits &= bits - 1;
@@ -236,8 +275,10 @@ __global__ void __launch_bounds__(BB, 4) k_bpass(BArgs a) {
                 continue;
             }
             const int nact = compact_groups<LPR, NV>(p, act, s_gp[wib], s_gi[wib], lane);
-            upd += scatter_lanes(a.R, a.V, nxt, nb, deg, s_gp[wib], s_gi[wib], nact, lane);
+            if (nact > DENSE_GROUPS) upd += scatter_rowpar<LPR, NV>(a.R, a.V, nxt, nb, deg, p, act, lane);
+            else upd += scatter_lanes(a.R, a.V, nxt, nb, deg, s_gp[wib], s_gi[wib], nact, lane);
             __syncwarp();
+        }
         }
     }
     __shared__ ull s_v[BB / 32], s_e[BB / 32], s_u[BB / 32], s_c[BB / 32];
@@ -276,11 +317,12 @@ __global__ void __launch_bounds__(BB) k_bhub(BArgs a) {
         bool act[NV];
 #pragma unroll
         for (int k = 0; k < NV; k++) {
-            p[k] = lane < LPR ? a.P[(size_t)sg.slot * a.V + j0 + LPR * k] : make_float4(0.f, 0.f, 0.f, 0.f);
+            p[k] = a.P[(size_t)sg.slot * a.V + j0 + LPR * k];
             act[k] = nonzero(p[k]);
         }
         const int nact = compact_groups<LPR, NV>(p, act, s_gp[wib], s_gi[wib], lane);
-        upd += scatter_lanes(a.R, a.V, nxt, sg.nb, sg.len, s_gp[wib], s_gi[wib], nact, lane);
+        if (nact > DENSE_GROUPS) upd += scatter_rowpar<LPR, NV>(a.R, a.V, nxt, sg.nb, sg.len, p, act, lane);
+        else upd += scatter_lanes(a.R, a.V, nxt, sg.nb, sg.len, s_gp[wib], s_gi[wib], nact, lane);
         __syncwarp();
     }
     __shared__ ull s_u[BB / 32];
