@@ -67,11 +67,17 @@ __global__ void __launch_bounds__(WB) k_wpass(WArgs a) {
     uint32_t* cur = a.touched[par];
     uint32_t* nxt = a.touched[par ^ 1];
     ull pv = 0, pe = 0;
-    for (long long w = gw; w < a.words; w += nwarps) {
-        const uint32_t bits = cur[w];
-        if (!bits) continue;
-        __syncwarp();
-        if (lane == 0) cur[w] = 0;
+    for (long long w0 = gw * 32; w0 < a.words; w0 += nwarps * 32) {
+        // 32 words per step, one per lane; then the warp takes the nonzero ones in turn
+        const long long wl = w0 + lane;
+        const uint32_t mine = wl < a.words ? cur[wl] : 0u;
+        if (mine) cur[wl] = 0;
+        unsigned nzw = __ballot_sync(FULL, mine != 0);
+        while (nzw) {
+        const int src = __ffs(nzw) - 1;
+        nzw &= nzw - 1;
+        const long long w = w0 + src;
+        const uint32_t bits = __shfl_sync(FULL, mine, src);
         const int v = (int)(w * 32 + lane);
         float d = 0.f;
         ull b0 = 0;
@@ -100,6 +106,7 @@ __global__ void __launch_bounds__(WB) k_wpass(WArgs a) {
                 red_add(a.r, u, f * __ldcs(a.wt + bb + i));
                 wmark(nxt, u);
             }
+        }
         }
     }
     __shared__ ull s_v[WB / 32], s_e[WB / 32];
