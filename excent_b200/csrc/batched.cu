@@ -114,6 +114,10 @@ __device__ __forceinline__ ull scatter_rowpar(float4* R, int V, uint32_t* nxt, c
     ull upd = 0;
     for (unsigned e0 = 0; e0 < deg; e0 += 32) {
         const int ul = e0 + lane < deg ? ld_edge(nb + e0 + lane) : -1;
+        if (ul >= 0) {   // each lane marks its own entry's target, all 32 at once
+            const uint32_t bit = 1u << (ul & 31);
+            if (!(nxt[ul >> 5] & bit)) atomicOr(&nxt[ul >> 5], bit);
+        }
         const unsigned cnt = min(32u, deg - e0);
         for (unsigned g = 0; g < cnt; g += RPW) {
             const int u = __shfl_sync(FULL, ul, (int)g + sub);
@@ -122,10 +126,6 @@ __device__ __forceinline__ ull scatter_rowpar(float4* R, int V, uint32_t* nxt, c
 #pragma unroll
                 for (int k = 0; k < NV; k++)
                     if (act[k]) { red_add(row, j0 + LPR * k, p[k]); upd++; }
-                if (j0 == 0) {
-                    const uint32_t bit = 1u << (u & 31);
-                    if (!(nxt[u >> 5] & bit)) atomicOr(&nxt[u >> 5], bit);
-                }
             }
         }
     }
