@@ -132,7 +132,7 @@ __device__ __forceinline__ ull scatter_rowpar(float4* R, int V, uint32_t* nxt, c
     return upd;
 }
 
-// Rows with more active 16-byte groups than this scatter over their groups.
+// Segments of rows with more active 16-byte groups than this scatter over their groups.
 static constexpr int DENSE_GROUPS = 16;
 
 // Compact the active groups of a row held by lanes j0 + LPR * k (k < NV) into
@@ -274,9 +274,9 @@ __global__ void __launch_bounds__(BB, 4) k_bpass(BArgs a) {
                 }
                 continue;
             }
+            // (lists up to BHUB_MIN: lanes over entries measured faster here at any density)
             const int nact = compact_groups<LPR, NV>(p, act, s_gp[wib], s_gi[wib], lane);
-            if (nact > DENSE_GROUPS) upd += scatter_rowpar<LPR, NV>(a.R, a.V, nxt, nb, deg, p, act, lane);
-            else upd += scatter_lanes(a.R, a.V, nxt, nb, deg, s_gp[wib], s_gi[wib], nact, lane);
+            upd += scatter_lanes(a.R, a.V, nxt, nb, deg, s_gp[wib], s_gi[wib], nact, lane);
             __syncwarp();
         }
         }
