@@ -64,8 +64,8 @@ __global__ void __launch_bounds__(WB) k_wpass(WArgs a) {
     const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     const int par = a.ctrl->pass & 1;
-    uint32_t* cur = a.touched[par];
-    uint32_t* nxt = a.touched[par ^ 1];
+    uint32_t* cur = par ? a.touched[1] : a.touched[0];   // no run-time index into the parameters
+    uint32_t* nxt = par ? a.touched[0] : a.touched[1];
     ull pv = 0, pe = 0;
     for (long long w0 = gw * 32; w0 < a.words; w0 += nwarps * 32) {
         // 32 words per step, one per lane; then the warp takes the nonzero ones in turn

@@ -167,8 +167,8 @@ __global__ void __launch_bounds__(BB, 4) k_bpass(BArgs a) {
     __shared__ float4 s_gp[BB / 32][LPR * NV];
     __shared__ int s_gi[BB / 32][LPR * NV];
     const int par = a.ctrl->pass & 1;
-    uint32_t* cur = a.touched[par];
-    uint32_t* nxt = a.touched[par ^ 1];
+    uint32_t* cur = par ? a.touched[1] : a.touched[0];   // no run-time index into the parameters
+    uint32_t* nxt = par ? a.touched[0] : a.touched[1];
     ull pushed_v = 0, pushed_e = 0, upd = 0, checked = 0;
     float4 eps[NV];
 #pragma unroll
@@ -305,7 +305,7 @@ __global__ void __launch_bounds__(BB) k_bhub(BArgs a) {
     const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     const int par = a.ctrl->pass & 1;
-    uint32_t* nxt = a.touched[par ^ 1];
+    uint32_t* nxt = par ? a.touched[0] : a.touched[1];
     ull nseg = a.ctrl->hub_segs[par];
     if (nseg > a.seg_cap) nseg = a.seg_cap;
     __shared__ float4 s_gp[BB / 32][LPR * NV];
