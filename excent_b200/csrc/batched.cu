@@ -173,17 +173,17 @@ __global__ void __launch_bounds__(BB, 4) k_bpass(BArgs a) {
     float4 eps[NV];
 #pragma unroll
     for (int k = 0; k < NV; k++) eps[k] = a.eps[j0 + LPR * k];
-    for (long long j0 = 0; gw + j0 * nwarps < a.words; j0 += 32) {
+    for (long long jw = 0; gw + jw * nwarps < a.words; jw += 32) {
         // warp gw owns words gw + j * nwarps (interleaved, so dense regions spread over all
         // warps); it reads 32 of them per step, one per lane, then walks the nonzero ones
-        const long long wl = gw + (j0 + lane) * nwarps;
+        const long long wl = gw + (jw + lane) * nwarps;
         const uint32_t mine = wl < a.words ? cur[wl] : 0u;
         if (mine) { cur[wl] = 0; checked += __popc(mine); }
         unsigned nzw = __ballot_sync(FULL, mine != 0);
         while (nzw) {
         const int src = __ffs(nzw) - 1;
         nzw &= nzw - 1;
-        const long long w = gw + (j0 + src) * nwarps;
+        const long long w = gw + (jw + src) * nwarps;
         uint32_t bits = __shfl_sync(FULL, mine, src);
         while (bits) {
             const int b = __ffs(bits) - 1;
