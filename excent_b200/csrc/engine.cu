@@ -203,40 +203,53 @@ __global__ void __launch_bounds__(BLOCK) k_snapshot(SnapArgs a) {
         const int nw = (int)min((long long)SNAP_GROUP, (long long)a.words - w0);
         uint32_t myb = 0;
         ull mydeg = 0;
-#pragma unroll 4
-        for (int j = 0; j < SNAP_GROUP; j++) {
-            if (j >= nw) break;
-            const long long v = (w0 + j) * 32 + lane;
-            bool pend = false;
-            if (v < a.n) {
-                T rv = r[v];
-                if (a.v1) {  // FP64 normalisation: drop the v1 component the push cannot remove
-                    const float q = a.v1[v];
-                    float* rp = reinterpret_cast<float*>(r + v) + (L == 1 ? 0 : a.ev);
-                    float re;
-                    if constexpr (L == 4) re = a.ev == 0 ? rv.x : a.ev == 1 ? rv.y : rv.z;
-                    else re = rv;
-                    if (evc != 0.0) {
-                        re = (float)((double)re - evc * (double)q);
-                        *rp = re;
-                        if constexpr (L == 4) { if (a.ev == 0) rv.x = re; else if (a.ev == 1) rv.y = re; else rv.z = re; }
-                        else rv = re;
-                    }
-                    evd += (double)re * (double)q;
-                }
-                if constexpr (L == 1) rs0 += fabs((double)rv);
-                else {
-                    rs0 += fabs((double)rv.x);
-                    rs1 += fabs((double)rv.y);
-                    rs2 += fabs((double)rv.z);
-                }
-                pend = pending_of(rv, a.M);
-                if (a.trace && pend) a.trace[v]++;
-                if (a.hot && pend && bit_of(a.hot, v)) { hp++; pend = false; }
-                if (pend) mydeg += a.idx[v + 1] - a.idx[v];
+        for (int j4 = 0; j4 < nw; j4 += 4) {
+            // four words' residuals (and v1 entries) in flight before they are examined
+            T rq[4];
+            float qq[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const long long v = (w0 + j4 + k) * 32 + lane;
+                const bool in = j4 + k < nw && v < a.n;
+                if (in) rq[k] = r[v];
+                qq[k] = in && a.v1 ? a.v1[v] : 0.f;
             }
-            const uint32_t b = __ballot_sync(FULL, pend);
-            if (lane == j) myb = b;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int j = j4 + k;
+                if (j >= nw) break;
+                const long long v = (w0 + j) * 32 + lane;
+                bool pend = false;
+                if (v < a.n) {
+                    T rv = rq[k];
+                    if (a.v1) {  // FP64 normalisation: drop the v1 component the push cannot remove
+                        const float q = qq[k];
+                        float* rp = reinterpret_cast<float*>(r + v) + (L == 1 ? 0 : a.ev);
+                        float re;
+                        if constexpr (L == 4) re = a.ev == 0 ? rv.x : a.ev == 1 ? rv.y : rv.z;
+                        else re = rv;
+                        if (evc != 0.0) {
+                            re = (float)((double)re - evc * (double)q);
+                            *rp = re;
+                            if constexpr (L == 4) { if (a.ev == 0) rv.x = re; else if (a.ev == 1) rv.y = re; else rv.z = re; }
+                            else rv = re;
+                        }
+                        evd += (double)re * (double)q;
+                    }
+                    if constexpr (L == 1) rs0 += fabs((double)rv);
+                    else {
+                        rs0 += fabs((double)rv.x);
+                        rs1 += fabs((double)rv.y);
+                        rs2 += fabs((double)rv.z);
+                    }
+                    pend = pending_of(rv, a.M);
+                    if (a.trace && pend) a.trace[v]++;
+                    if (a.hot && pend && bit_of(a.hot, v)) { hp++; pend = false; }
+                    if (pend) mydeg += a.idx[v + 1] - a.idx[v];
+                }
+                const uint32_t b = __ballot_sync(FULL, pend);
+                if (lane == j) myb = b;
+            }
         }
         if (lane < nw) a.bitmap[w0 + lane] = myb;
         const unsigned cl = lane < nw ? (unsigned)__popc(myb) : 0u;
