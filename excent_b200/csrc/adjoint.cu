@@ -67,18 +67,11 @@ __global__ void __launch_bounds__(WB) k_wpass(WArgs a) {
     uint32_t* cur = par ? a.touched[1] : a.touched[0];   // no run-time index into the parameters
     uint32_t* nxt = par ? a.touched[0] : a.touched[1];
     ull pv = 0, pe = 0;
-    for (long long jw = 0; gw + jw * nwarps < a.words; jw += 32) {
-        // warp gw owns words gw + j * nwarps; it reads 32 of them per step, one per lane,
-        // then takes the nonzero ones in turn
-        const long long wl = gw + (jw + lane) * nwarps;
-        const uint32_t mine = wl < a.words ? cur[wl] : 0u;
-        if (mine) cur[wl] = 0;
-        unsigned nzw = __ballot_sync(FULL, mine != 0);
-        while (nzw) {
-        const int src = __ffs(nzw) - 1;
-        nzw &= nzw - 1;
-        const long long w = gw + (jw + src) * nwarps;
-        const uint32_t bits = __shfl_sync(FULL, mine, src);
+    for (long long w = gw; w < a.words; w += nwarps) {
+        const uint32_t bits = cur[w];
+        if (!bits) continue;
+        __syncwarp();
+        if (lane == 0) cur[w] = 0;
         const int v = (int)(w * 32 + lane);
         float d = 0.f;
         ull b0 = 0;
@@ -107,7 +100,6 @@ __global__ void __launch_bounds__(WB) k_wpass(WArgs a) {
                 red_add(a.r, u, f * __ldcs(a.wt + bb + i));
                 wmark(nxt, u);
             }
-        }
         }
     }
     __shared__ ull s_v[WB / 32], s_e[WB / 32];
