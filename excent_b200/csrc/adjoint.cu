@@ -95,10 +95,21 @@ __global__ void __launch_bounds__(WB) k_wpass(WArgs a) {
             const ull bb = __shfl_sync(FULL, b0, sl);
             const unsigned dd = __shfl_sync(FULL, deg, sl);
             const float f = a.s * __shfl_sync(FULL, d, sl);
-            for (unsigned i = lane; i < dd; i += 32) {
-                const int u = ld_edge(a.adj + bb + i);
-                red_add(a.r, u, f * __ldcs(a.wt + bb + i));
-                wmark(nxt, u);
+            for (unsigned i0 = 0; i0 < dd; i0 += 128) {
+                int u[4];
+                float wt[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) {   // four entries per lane in flight
+                    const unsigned i = i0 + 32 * k + lane;
+                    u[k] = i < dd ? ld_edge(a.adj + bb + i) : -1;
+                    wt[k] = i < dd ? __ldcs(a.wt + bb + i) : 0.f;
+                }
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (u[k] >= 0) red_add(a.r, u[k], f * wt[k]);
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (u[k] >= 0) wmark(nxt, u[k]);
             }
         }
     }
