@@ -80,6 +80,8 @@ def parse():
     ap.add_argument("--ooc-measures", default="pr", help="comma-separated measures of the out-of-core run")
     ap.add_argument("--ooc-mode", default="pinned", choices=["pinned", "pipeline"],
                     help="which of this repo's out-of-core arms is the headline")
+    ap.add_argument("--ooc-pipeline", default="on", choices=["on", "off"],
+                    help="also run this repo's CLI with the reference's stream/gather pipeline")
     ap.add_argument("--ooc-ref", default="on", choices=["on", "off"], help="also run the reference CLI out of core")
     ap.add_argument("--batch-width", type=int, default=0, choices=[0, 32, 64, 128, 256],
                     help="batched PPR: fixed batch width instead of the autotuner's")
@@ -700,8 +702,9 @@ def run_ooc(a, world, rank, local, dist):
             elif measure != "pr":
                 return {"metric": "GTEPS (out of core)", "unavailable": f"measure {measure} is not part of this run"}
             arms = [("ours_pinned", K.CLI_PATH, ["--host-cache", "pinned", "--list-frac", str(a.list_frac),
-                                                 "--hub-order", a.hub_order]),
-                    ("ours", K.CLI_PATH, [])]
+                                                 "--hub-order", a.hub_order])]
+            if a.ooc_pipeline == "on":
+                arms.append(("ours", K.CLI_PATH, []))
             if a.ooc_ref == "on" and os.path.exists(ref_bin):
                 arms.append(("reference", ref_bin, []))
             for name, binary, extra in arms:
