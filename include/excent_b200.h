@@ -250,8 +250,10 @@ int excent_engine_host_pushed(excent_engine* e, unsigned long long* entries);
  * pending degrees) is at least pull_frac * m runs as a gather. It takes every
  * pending vertex (no concurrent updates in that pass), writes its per-entry
  * weight, then adds to each vertex the weights of its neighbours: the sum the
- * scatter would have added, without atomics. 0 turns it off (the default).
- * No reference counterpart: the reference always scatters. */
+ * scatter would have added, without atomics. 0 turns it off (the default; on
+ * R-MAT graphs a gather pass is a Jacobi step and the solve pushes more entries
+ * than it saves in atomics). Ignored while a host cache is set. No reference
+ * counterpart: the reference always scatters. */
 int excent_engine_set_pull(excent_engine* e, double pull_frac);
 
 /* FP64 eigenvector normalisation step: with the unit principal eigenvector
