@@ -299,6 +299,9 @@ def run_ours(a, world, rank, local, dist):
         "roofline": {"bound": "hbm", "kernel": "k_push + k_hub (one logical push per pass)",
                      "achieved": round(achieved, 1), "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": None,
+                     "traffic_note": "not measured in this run; an ncu capture of one scale-24 solve of this "
+                                     "command gave 398.7 GB of DRAM traffic for the push kernels against 837 GB "
+                                     "algorithmic (profiles/traffic_all_rmat24.md)",
                      "alg_bytes_per_solve": int(b_alg), "push_ms_per_solve": round(t_push * 1e3, 3),
                      "pass_ms_per_solve": round(t_all * 1e3, 3),
                      "pass_achieved_gbs": round((b_alg + snap_bytes) / t_all / 1e9, 1) if t_all else None,
