@@ -503,9 +503,17 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
             if ((SRC == SRC_TABLE || SRC == SRC_HUBS) && a.hcache && a.idx[v] >= a.cache_edges) hpushed += deg;
         }
         const bool large = act && deg > HUB_MIN;
+        // one queue reservation per warp for all its long lists (the counter is shared by the grid)
+        const unsigned nseg = large ? (unsigned)((deg + HUB_SEG - 1) / HUB_SEG) : 0u;
+        const unsigned sincl = warp_incl_scan(nseg, lane);
+        const unsigned stot = __shfl_sync(FULL, sincl, 31);
+        ull sbase = 0;
+        if (stot) {
+            if (lane == 0) sbase = atomicAdd(a.hub_cnt, (ull)stot);
+            sbase = __shfl_sync(FULL, sbase, 0);
+        }
         if (large) {
-            const unsigned nseg = (unsigned)((deg + HUB_SEG - 1) / HUB_SEG);
-            const ull base = atomicAdd(a.hub_cnt, (ull)nseg);
+            const ull base = sbase + (sincl - nseg);
             if (base + nseg <= a.hub_cap) {
                 HubSeg* q = a.hubq + base;
                 for (unsigned s = 0; s < nseg; s++) {
