@@ -4,8 +4,8 @@
 
 CUDA sources are compiled with nvcc for `-gencode arch=compute_100a,code=sm_100a`
 (cross-compiles without a GPU); host C++ with g++ and OpenMP. Objects go to
-excent_b200/_build/, the library to excent_b200/libexcent_b200.so and the CLI to
-excent_b200/bin/excent (rpath $ORIGIN/..).
+excent_b200/_build/, the library to excent_b200/libexcent_b200.so and the tools to
+excent_b200/bin/ (excent, excent_params; rpath $ORIGIN/..).
 """
 from __future__ import annotations
 
@@ -24,6 +24,7 @@ INC = os.path.join(ROOT, "include")
 OBJ = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libexcent_b200.so")
 CLI = os.path.join(PKG, "bin", "excent")
+TOOLS = {"cli_main": CLI, "cli_params": os.path.join(PKG, "bin", "excent_params")}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 
@@ -86,9 +87,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
         cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-Xcompiler", "-fopenmp", "-o", LIB, *lib_objs,
                "-lgomp"]
         subprocess.run(cmd, check=True)
-    if cli_objs and (force or _stale(CLI, cli_objs + [LIB])):
-        cmd = ["g++", "-o", CLI, *cli_objs, "-L" + PKG, "-lexcent_b200", "-Wl,-rpath,$ORIGIN/..", "-fopenmp"]
-        subprocess.run(cmd, check=True)
+    for obj in cli_objs:   # one binary per cli_*.cpp
+        out = TOOLS[os.path.basename(obj).rsplit(".", 1)[0]]
+        if force or _stale(out, [obj, LIB]):
+            cmd = ["g++", "-o", out, obj, "-L" + PKG, "-lexcent_b200", "-Wl,-rpath,$ORIGIN/..", "-fopenmp"]
+            subprocess.run(cmd, check=True)
     return LIB
 
 

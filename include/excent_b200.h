@@ -352,6 +352,10 @@ double excent_tau(double t_stream, const double* t_g, const double* f);
  * --device-loop). Prints the reference's stdout lines; returns the process
  * exit code (0, or 1 on a usage or run error). */
 int excent_cli_main(int argc, char** argv);
+/* bin/excent_params graph.egr out.env [--device N]: lambda1, the Katz and
+ * eigenvector fixed-point means (FP64, on the GPU) and the .env file the CLI
+ * reads (tools/excent_params.cu:73-172: same arguments, stdout lines, keys). */
+int excent_params_main(int argc, char** argv);
 
 /* ------------------------------------------------------------ batched solves */
 

@@ -143,3 +143,24 @@ def test_cli_tau_calibration_and_cache_file(rmat14, tmp_path):
     assert abs(float(tau) - float(m.group(1))) < 1e-3
     out2 = run(CLI, [p, "--measure", "pr", "--cache", "none"], tmp_path)
     assert "measured earlier on this machine" in out2
+
+
+def test_params_tool_reproduces_the_sample_env(tmp_path):
+    """bin/excent_params writes the sample graph's given constants: the
+    reference's only known answer (datasets/sample/sample.env), and the
+    reference's own tool on the same file when it was built."""
+    tool = os.path.join(os.path.dirname(CLI), "excent_params")
+    out = run(tool, [SAMPLE, str(tmp_path / "s.env")], tmp_path)
+    assert re.search(r"^lambda1 = [0-9.]+ after \d+ power iterations", out, re.M), out
+    got = read_env(str(tmp_path / "s.env"))
+    want = read_env(os.path.join(GOLDEN, "sample.env"))
+    assert abs(float(got["LAMBDA"]) - float(want["LAMBDA"])) <= 1e-9 * float(want["LAMBDA"])
+    for k in ("ALPHA", "BETA", "EPS_PR", "EPS_KATZ", "EPS_EV"):
+        assert got[k] == want[k], (k, got[k], want[k])
+    ref_tool = os.path.join(O.REF_DIR, "excent_params")
+    if os.path.exists(ref_tool):
+        run(ref_tool, [SAMPLE, str(tmp_path / "r.env")], tmp_path)
+        ref = read_env(str(tmp_path / "r.env"))
+        for k in ("ALPHA", "BETA", "EPS_PR", "EPS_KATZ", "EPS_EV"):
+            assert got[k] == ref[k], (k, got[k], ref[k])
+

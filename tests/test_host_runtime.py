@@ -306,3 +306,28 @@ def test_cli_bad_file_is_an_error(tmp_path):
     p.write_bytes(np.array([100, 50], dtype="<i4").tobytes())
     r = subprocess.run([CLI, str(p), "--measure", "pr"], capture_output=True, text=True)
     assert r.returncode == 1 and "truncated" in r.stderr
+
+
+PARAMS = os.path.join(os.path.dirname(K.CLI_PATH), "excent_params")
+REF_PARAMS = os.path.join(O.REF_DIR, "excent_params")
+
+
+def test_params_tool_usage_matches_reference():
+    ours = subprocess.run([PARAMS], capture_output=True, text=True)
+    assert ours.returncode == 1 and "usage:" in ours.stderr
+    if not os.path.exists(REF_PARAMS):
+        pytest.skip("reference tool not built")
+    ref = subprocess.run([REF_PARAMS], capture_output=True, text=True)
+    assert ref.returncode == 1
+    assert ours.stderr.replace(PARAMS, "X") == ref.stderr.replace(REF_PARAMS, "X")
+
+
+def test_params_tool_symmetry_check_before_any_gpu_work(tmp_path):
+    """An asymmetric graph is rejected by the sampled symmetry check, with the
+    reference tool's message, before the device is touched."""
+    n, idx, adj = O.rmat_graph(10, 8, 3, symmetric=False)
+    p = str(tmp_path / "d.egr")
+    O.write_egr(p, idx, adj)
+    ours = subprocess.run([PARAMS, p, str(tmp_path / "d.env")], capture_output=True, text=True)
+    assert ours.returncode == 1 and "graph is not symmetric" in ours.stderr
+    assert ours.stdout.startswith(f"graph: n={n} m={len(adj)}")
