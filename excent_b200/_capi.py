@@ -128,6 +128,7 @@ PROTOS = [
     ("excent_tau", C.c_double, [C.c_double, vp, vp]),
     ("excent_cli_main", C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
     ("excent_params_main", C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
+    ("excent_reference_main", C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
     ("excent_rmat_generate", C.c_int, [C.c_int, C.c_int, C.c_int, u64, C.c_double, C.c_double, C.c_double,
                                        C.c_int, C.c_int, C.POINTER(vp)]),
     ("excent_ppr_fp64", C.c_int, [C.c_int, C.c_int, vp, vp, C.c_double, C.c_int, vp, vp, C.c_double, C.c_int, vp,

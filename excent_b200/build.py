@@ -5,7 +5,7 @@
 CUDA sources are compiled with nvcc for `-gencode arch=compute_100a,code=sm_100a`
 (cross-compiles without a GPU); host C++ with g++ and OpenMP. Objects go to
 excent_b200/_build/, the library to excent_b200/libexcent_b200.so and the tools to
-excent_b200/bin/ (excent, excent_params; rpath $ORIGIN/..).
+excent_b200/bin/ (excent, excent_params, excent_reference; rpath $ORIGIN/..).
 """
 from __future__ import annotations
 
@@ -24,7 +24,8 @@ INC = os.path.join(ROOT, "include")
 OBJ = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libexcent_b200.so")
 CLI = os.path.join(PKG, "bin", "excent")
-TOOLS = {"cli_main": CLI, "cli_params": os.path.join(PKG, "bin", "excent_params")}
+TOOLS = {"cli_main": CLI, "cli_params": os.path.join(PKG, "bin", "excent_params"),
+         "cli_reference": os.path.join(PKG, "bin", "excent_reference")}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 

@@ -356,6 +356,10 @@ int excent_cli_main(int argc, char** argv);
  * eigenvector fixed-point means (FP64, on the GPU) and the .env file the CLI
  * reads (tools/excent_params.cu:73-172: same arguments, stdout lines, keys). */
 int excent_params_main(int argc, char** argv);
+/* bin/excent_reference: the FP64 oracle of a graph on the GPU (ref.bin of n
+ * doubles) and --compare / --rank / --compare-dumps of float32 dumps against
+ * it (tools/centrality_reference.cu:71-214: same modes, files and lines). */
+int excent_reference_main(int argc, char** argv);
 
 /* ------------------------------------------------------------ batched solves */
 

@@ -164,3 +164,18 @@ def test_params_tool_reproduces_the_sample_env(tmp_path):
         for k in ("ALPHA", "BETA", "EPS_PR", "EPS_KATZ", "EPS_EV"):
             assert got[k] == ref[k], (k, got[k], ref[k])
 
+
+
+@pytest.mark.parametrize("measure", ["pr", "katz", "ev"])
+def test_reference_tool_solve_matches_the_golden_fp64(tmp_path, measure):
+    """bin/excent_reference's FP64 solve on the GPU against the golden FP64
+    solution the reference's own tool wrote for the sample graph."""
+    env = read_env(os.path.join(GOLDEN, "sample.env"))
+    tool = os.path.join(os.path.dirname(CLI), "excent_reference")
+    extra = ["--alpha", env["ALPHA"]] if measure == "katz" else []
+    out = run(tool, [SAMPLE, measure, str(tmp_path / "r.bin"), *extra], tmp_path)
+    assert out.startswith(f"reference {measure}:"), out
+    got = np.fromfile(str(tmp_path / "r.bin"), dtype=np.float64)
+    want = np.fromfile(os.path.join(GOLDEN, f"sample_ref_{measure}.f64"), dtype=np.float64)
+    assert got.shape == want.shape
+    assert np.abs(got - want).max() <= 1e-8 * np.abs(want).max()

@@ -331,3 +331,33 @@ def test_params_tool_symmetry_check_before_any_gpu_work(tmp_path):
     ours = subprocess.run([PARAMS, p, str(tmp_path / "d.env")], capture_output=True, text=True)
     assert ours.returncode == 1 and "graph is not symmetric" in ours.stderr
     assert ours.stdout.startswith(f"graph: n={n} m={len(adj)}")
+
+
+REFTOOL = os.path.join(os.path.dirname(K.CLI_PATH), "excent_reference")
+REF_REFTOOL = os.path.join(O.REF_DIR, "centrality_reference")
+
+
+@pytest.mark.parametrize("mode", ["--compare", "--rank"])
+@pytest.mark.parametrize("measure,dump", [("pr", "sample_excent_pr_pr.f32"), ("katz", "sample_excent_katz_katz.f32"),
+                                          ("ev", "sample_excent_ev_ev.f32"), ("ev", "sample_excent_all_ev.f32")])
+def test_reference_tool_comparison_matches_reference(mode, measure, dump):
+    """--compare / --rank of the reference engine's golden dumps against the
+    golden FP64 solution: the same line as the reference's own tool (CPU only)."""
+    args = [mode, measure, os.path.join(GOLDEN, f"sample_ref_{measure}.f64"), os.path.join(GOLDEN, dump)]
+    ours = subprocess.run([REFTOOL, *args], capture_output=True, text=True)
+    assert ours.returncode == 0, ours.stderr
+    assert ours.stdout.startswith(f"{measure}:")
+    if not os.path.exists(REF_REFTOOL):
+        pytest.skip("reference tool not built")
+    ref = subprocess.run([REF_REFTOOL, *args], capture_output=True, text=True)
+    assert ref.returncode == 0
+    assert ours.stdout == ref.stdout
+
+
+def test_reference_tool_usage_matches_reference():
+    ours = subprocess.run([REFTOOL], capture_output=True, text=True)
+    assert ours.returncode == 1
+    if not os.path.exists(REF_REFTOOL):
+        pytest.skip("reference tool not built")
+    ref = subprocess.run([REF_REFTOOL], capture_output=True, text=True)
+    assert ours.stderr.replace(REFTOOL, "X") == ref.stderr.replace(REF_REFTOOL, "X")
