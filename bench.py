@@ -85,6 +85,8 @@ def parse():
     ap.add_argument("--ooc-ref", default="on", choices=["on", "off"], help="also run the reference CLI out of core")
     ap.add_argument("--batch-width", type=int, default=0, choices=[0, 32, 64, 128, 256],
                     help="batched PPR: fixed batch width instead of the autotuner's")
+    ap.add_argument("--dense-groups", type=int, default=-1,
+                    help="batched PPR: active-group threshold of the group-parallel hub scatter (-1: default)")
     ap.add_argument("--greedy", default="off", choices=["on", "off"], help="with --batch-width: greedy row push")
     ap.add_argument("--list-frac", type=float, default=0.5,
                     help="per-chunk list/range rule of the device loop (the reference's --list-frac)")
@@ -353,6 +355,8 @@ def run_ppr(a, world, rank, local, dist):
     use_graph = not a.no_graph
     b = X.Batch(n, m, di, da, best, "ppr", d, device=local)
     b.set_greedy(greedy)
+    if a.dense_groups >= 0:
+        b.set_dense(a.dense_groups)
     st = torch.cuda.ExternalStream(b.stream())
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     b.seed(qs[:best], vals[:best], eps)   # warm-up (graph build)

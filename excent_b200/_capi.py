@@ -77,6 +77,7 @@ PROTOS = [
     ("excent_batch_stream", C.c_int, [vp, C.POINTER(vp)]),
     ("excent_batch_launches", C.c_int, [vp, u64p]),
     ("excent_batch_set_greedy", C.c_int, [vp, C.c_int]),
+    ("excent_batch_set_dense", C.c_int, [vp, C.c_int]),
     ("excent_batch_autotune", C.c_int, [C.c_int, C.c_int, u64, vp, vp, C.c_int, C.c_double, C.c_int, vp, vp, vp, vp,
                                         C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), f64p]),
     ("excent_engine_stats", C.c_int, [vp, C.POINTER(Stats), C.POINTER(PassLog), C.c_int]),

@@ -69,6 +69,7 @@ struct BArgs {
     ull seg_cap;
     BCtrl* ctrl;
     int greedy;               // take every nonzero lane of a pushed row, not only the pending ones
+    int dense;                // hub segments of rows with more active groups scatter over the groups
 };
 
 __device__ __forceinline__ float take_lane(float* rp, float rv, float eps) {
@@ -132,7 +133,7 @@ __device__ __forceinline__ ull scatter_rowpar(float4* R, int V, uint32_t* nxt, c
     return upd;
 }
 
-// Segments of rows with more active 16-byte groups than this scatter over their groups.
+// Default: segments of rows with more active 16-byte groups than this scatter over their groups.
 static constexpr int DENSE_GROUPS = 16;
 
 // Compact the active groups of a row held by lanes j0 + LPR * k (k < NV) into
@@ -322,7 +323,7 @@ __global__ void __launch_bounds__(BB) k_bhub(BArgs a) {
             act[k] = nonzero(p[k]);
         }
         const int nact = compact_groups<LPR, NV>(p, act, s_gp[wib], s_gi[wib], lane);
-        if (nact > DENSE_GROUPS) upd += scatter_rowpar<LPR, NV>(a.R, a.V, nxt, sg.nb, sg.len, p, act, lane);
+        if (nact > a.dense) upd += scatter_rowpar<LPR, NV>(a.R, a.V, nxt, sg.nb, sg.len, p, act, lane);
         else upd += scatter_lanes(a.R, a.V, nxt, sg.nb, sg.len, s_gp[wib], s_gi[wib], nact, lane);
         __syncwarp();
     }
@@ -408,6 +409,7 @@ struct excent_batch {
     int grid = 0;
     ull launches = 0;
     int greedy = 1;
+    int dense = DENSE_GROUPS;   // see excent_batch_set_dense
 };
 
 static void batch_free(excent_batch* b) {
@@ -436,6 +438,7 @@ static BArgs bargs(excent_batch* b) {
     a.P = b->d_P; a.prow_cap = b->prow_cap; a.seg = b->d_seg; a.seg_cap = b->seg_cap;
     a.ctrl = b->d_ctrl;
     a.greedy = b->greedy;
+    a.dense = b->dense;
     return a;
 }
 
@@ -647,6 +650,15 @@ extern "C" int excent_batch_read(excent_batch* b, int lane, int residual, float*
     EX_CUDA(cudaGetLastError());
     EX_CUDA(cudaMemcpyAsync(out, b->d_col, (size_t)b->n * sizeof(float), cudaMemcpyDeviceToHost, b->st));
     EX_CUDA(cudaStreamSynchronize(b->st));
+    return EXCENT_OK;
+}
+
+extern "C" int excent_batch_set_dense(excent_batch* b, int groups) {
+    EX_CHECK_ARG(b && groups >= 0, "bad argument");
+    b->dense = groups;
+    if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
+    if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+    b->graph_max = -1;
     return EXCENT_OK;
 }
 
