@@ -380,7 +380,7 @@ class Batch:
         call("excent_batch_seed", self.h, nq, _ptr(off), _ptr(vids) if len(vids) else None,
              _ptr(vals) if len(vals) else None, _ptr(e))
 
-    def set_dense(self, groups=16):
+    def set_dense(self, groups=4):
         """Hub segments of rows with more active 16-byte groups than this scatter over the groups."""
         call("excent_batch_set_dense", self.h, int(groups))
 

@@ -134,7 +134,7 @@ __device__ __forceinline__ ull scatter_rowpar(float4* R, int V, uint32_t* nxt, c
 }
 
 // Default: segments of rows with more active 16-byte groups than this scatter over their groups.
-static constexpr int DENSE_GROUPS = 16;
+static constexpr int DENSE_GROUPS = 4;
 
 // Compact the active groups of a row held by lanes j0 + LPR * k (k < NV) into
 // the warp's shared lists; returns their count (warp-uniform).

@@ -397,7 +397,7 @@ int excent_batch_set_greedy(excent_batch* b, int greedy);
 /* Segments of lists longer than 512 entries whose row has more than `groups`
  * active 16-byte lane groups scatter over the groups (each reduction covers a
  * contiguous stretch of the target row); sparser ones with the lanes over the
- * entries. Default 16. */
+ * entries. Default 4 (measured: 4 and 8 best, 64 slowest, at B = 256). */
 int excent_batch_set_dense(excent_batch* b, int groups);
 /* Autotuner: time one batch of min(B, nq) of the given queries (seeded as
  * in excent_batch_seed) at each width B in {32, 64, 128, 256}, with the
