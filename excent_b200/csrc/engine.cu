@@ -1913,7 +1913,7 @@ extern "C" int excent_device_info(int device, excent_device_info_t* out) {
 
 extern "C" int excent_engine_set_hub_targets(excent_engine* e, int k) {
     EX_CHECK_ARG(e && k >= 0, "bad argument");
-    const int kmax = e->L == 1 ? 8192 : 2048;   // 32 KiB of shared accumulators per block
+    const int kmax = e->L == 1 ? 16384 : 4096;   // 64 KiB of shared accumulators per block
     EX_CHECK_ARG(k <= kmax, "at most %d hub targets for this layout", kmax);
     EX_CHECK_ARG(k <= e->n, "more hub targets than vertices");
     EX_CUDA(cudaSetDevice(e->dev));
@@ -1945,12 +1945,30 @@ extern "C" int excent_engine_set_hub_targets(excent_engine* e, int k) {
         if (!e->d_hub_id) EX_ALLOC(e->d_hub_id, (size_t)kmax * sizeof(int));
         EX_CUDA(cudaMemcpy(e->d_hub_id, ids.data(), (size_t)k * sizeof(int), cudaMemcpyHostToDevice));
         e->hub_k = k;
+        if ((size_t)k * sizeof(int) > 48 * 1024)   // the encoder keeps the sorted ids in shared memory
+            EX_CUDA(cudaFuncSetAttribute(k_hub_encode, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)((size_t)k * sizeof(int))));
         for (int c = 0; c < e->nc; c++)   // chunks loaded so far; later loads encode themselves
             if (e->loaded[c] && e->ce[c + 1] <= e->cache_edges) hub_encode(e, e->ce[c], e->ce[c + 1], e->s_main);
         EX_CUDA(cudaStreamSynchronize(e->s_main));
         EX_CUDA(cudaGetLastError());
     }
     const size_t smem = hub_smem(e);
+    if (smem > 48 * 1024) {   // above the default dynamic shared memory limit: opt in, per kernel
+        const int sz = (int)smem;
+        cudaFuncSetAttribute(k_push<1, SRC_TABLE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz);
+        cudaFuncSetAttribute(k_push<1, SRC_CHUNK>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz);
+        cudaFuncSetAttribute(k_push<1, SRC_GATHER>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz);
+        cudaFuncSetAttribute(k_push<1, SRC_HOT>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz);
+        cudaFuncSetAttribute(k_push<1, SRC_HUBS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz);
+        cudaFuncSetAttribute(k_push<4, SRC_TABLE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz);
+        cudaFuncSetAttribute(k_push<4, SRC_CHUNK>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz);
+        cudaFuncSetAttribute(k_push<4, SRC_GATHER>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz);
+        cudaFuncSetAttribute(k_push<4, SRC_HOT>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz);
+        cudaFuncSetAttribute(k_push<4, SRC_HUBS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz);
+        cudaFuncSetAttribute(k_hub<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz);
+        EX_CUDA(cudaFuncSetAttribute(k_hub<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+    }
     int occ = 0;
     if (e->L == 1) EX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_push<1, SRC_TABLE>, BLOCK, smem));
     else EX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_push<4, SRC_TABLE>, BLOCK, smem));
