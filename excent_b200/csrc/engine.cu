@@ -1913,7 +1913,7 @@ extern "C" int excent_device_info(int device, excent_device_info_t* out) {
 
 extern "C" int excent_engine_set_hub_targets(excent_engine* e, int k) {
     EX_CHECK_ARG(e && k >= 0, "bad argument");
-    const int kmax = e->L == 1 ? 16384 : 4096;   // 64 KiB of shared accumulators per block
+    const int kmax = e->L == 1 ? 32768 : 8192;   // 128 KiB of shared accumulators per block
     EX_CHECK_ARG(k <= kmax, "at most %d hub targets for this layout", kmax);
     EX_CHECK_ARG(k <= e->n, "more hub targets than vertices");
     EX_CUDA(cudaSetDevice(e->dev));

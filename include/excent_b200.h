@@ -219,7 +219,7 @@ int excent_engine_read_trace(excent_engine* e, uint16_t* out);
  * contributions to those targets in shared memory and add them to the
  * residuals once per block instead of once per entry (the hubs of a power-law
  * graph receive a large share of all entries, and same-address reductions
- * serialise in L2). k <= 16384 (one measure) or 4096 (float4 layout); 0 turns
+ * serialise in L2). k <= 32768 (one measure) or 8192 (float4 layout); 0 turns
  * it off and restores plain ids. Call after the cache is reserved: chunks
  * loaded so far are rewritten now, later loads (load_cache, upload_device,
  * cache-filling streamed pushes) as they land; reserving the cache again
