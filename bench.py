@@ -94,8 +94,8 @@ def parse():
     ap.add_argument("--hub-order", default="first", choices=["first", "last", "table"],
                     help="where the high-degree lists go in each pass of the device loop")
     ap.add_argument("--hub-targets", type=int, default=-1,
-                    help="shared-memory aggregation of the k highest-degree targets (0: off; -1: 8192 for "
-                         "one measure, 2048 for all)")
+                    help="shared-memory aggregation of the k highest-degree targets (0: off; -1: 16384 for "
+                         "one measure, 4096 for all)")
     ap.add_argument("--ev-init", default="fp64", choices=["fp64", "reference"],
                     help="eigenvector initial residual from the FP64 lambda1 (default) or from lambda1 rounded to "
                          "float as the reference does")
@@ -202,7 +202,7 @@ def run_ours(a, world, rank, local, dist):
     if v1 is not None and a.ev_project == "on":
         eng.ev_project(v1)
     eng.set_pull(a.pull_frac)
-    hub_k = a.hub_targets if a.hub_targets >= 0 else min(8192 if nm == 1 else 2048, n)
+    hub_k = a.hub_targets if a.hub_targets >= 0 else min(16384 if nm == 1 else 4096, n)
     eng.set_hub_targets(hub_k)
     eng.set_hub_order(a.hub_order)
     use_graph = not a.no_graph

@@ -237,7 +237,7 @@ static int run(const Options& o) {
         }
         for (int c = 0; c < n_resident; c++) { resident[c] = 1; resident_edges += chunks[c].edges(); }
         if (n_resident > 0) {   // shared-memory sums for the top-degree targets of cached pushes
-            const int k = o.hub_targets < 0 ? std::min(M.nm == 1 ? 8192 : 2048, n) : o.hub_targets;
+            const int k = o.hub_targets < 0 ? std::min(M.nm == 1 ? 16384 : 4096, n) : o.hub_targets;
             if (k > 0 && excent_engine_set_hub_targets(e, k) != EXCENT_OK)   // an optimisation: go on without it
                 fprintf(stderr, "excent: hub targets off (%s)\n", excent_last_error());
         }
