@@ -466,12 +466,12 @@ __device__ __forceinline__ long long item_total(const PushArgs& a) {
 
 // Push kernel (persistent grid, warp tiles of 32 items). Each lane takes one
 // item's residual (the push-time re-check and exchange of
-// src/excent.cu:109-112), then the warp dispatches by degree: lists of <= 32
-// entries are scattered edge-balanced across the warp (lane j handles the
-// j-th entry of the tile's concatenated lists), lists up to 2048 entries by
-// the whole warp with 128-bit index loads, longer lists are queued as
-// 2048-entry hub segments for k_hub. Residuals are added with red.global
-// (a float4 reduction per edge carries every measure of an `all` run).
+// src/excent.cu:109-112), then the warp dispatches by degree: lists of up to
+// HUB_MIN entries are scattered edge-balanced across the warp (lane j handles
+// the j-th entry of each 32-entry window of the tile's concatenated lists),
+// longer lists are queued as HUB_SEG-entry hub segments for k_hub. Residuals
+// are added with red.global (a float4 reduction per entry carries every
+// measure of an `all` run), or in the block's shared hub-target slots.
 template <int L, int SRC>
 __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
     typedef typename Lane<L>::T T;
@@ -577,7 +577,7 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
     }
 }
 
-// Hub segments queued by k_push: one warp per 2048-entry segment.
+// Hub segments queued by k_push: one warp per HUB_SEG-entry segment.
 template <int L>
 __global__ void __launch_bounds__(BLOCK) k_hub(void* rv, const HubSeg* q, const ull* hub_cnt, ull cap,
                                                const int* hub_id, int hub_k) {
