@@ -40,7 +40,6 @@ struct HubSeg {
 struct Ctrl {
     ull hotpend;
     ull pushed;        // adjacency entries pushed since init
-    ull hub_unused;
     ull items;         // work items of the cached push in this pass
     int pass;          // passes that pushed so far
     int done;          // 1 once a snapshot found nothing pending (or max passes)
