@@ -1602,8 +1602,12 @@ static void enqueue_pass(excent_engine* e, double list_frac, int max_passes, cud
     // collect the pass's residual and push it once; 0 = in table order with the rest
     const int order = e->hub_order && e->d_hubv && !e->hubv_stale ? e->hub_order : 0;
     auto hub_phase = [&]() {
-        if (e->L == 1) k_push<1, SRC_HUBS><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
-        else k_push<4, SRC_HUBS><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
+        // every list of SRC_HUBS is longer than HUB_MIN, so this push only takes and queues:
+        // no entry is scattered here and the hub-target slots are not needed
+        PushArgs ah = a;
+        ah.hub_k = 0;
+        if (e->L == 1) k_push<1, SRC_HUBS><<<e->grid_push, BLOCK, 0, st>>>(ah);
+        else k_push<4, SRC_HUBS><<<e->grid_push, BLOCK, 0, st>>>(ah);
         if (e->L == 1) k_hub<1><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
         else k_hub<4><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
         e->launches += 2;
