@@ -121,6 +121,7 @@ extern "C" int excent_params_fp64(int device, int n, const unsigned long long* d
     for (; pit < 5000; pit++) {
         k_pull64<<<wb, 256>>>(n, d_idx, d_adj, B.v[0], B.v[1], 0.0, 1.0, 0, nullptr);
         EX_TRY(norms(n, B.v[1], nullptr, B, G, &ss, nullptr, nullptr));
+        if (!(ss > 0)) EX_FAIL(EXCENT_ERR_ARG, "params: the graph has no edges (A x = 0), lambda1 is undefined");
         lam = std::sqrt(ss);
         k_scale64<<<G, 256>>>(n, B.v[1], 1.0 / lam, 0.0);
         std::swap(B.v[0], B.v[1]);

@@ -18,14 +18,17 @@
 // overlap on the GPU (two host threads, or two streams) race on it and must
 // be serialised by the caller.
 //
-// Host code cannot use the array's name as a device address. The first call
-// on each device (with that device current) looks the address up once with
-// cudaGetSymbolAddress; make that first call before any stream capture.
+// Host code cannot use the array's name as a device address. Every call looks
+// the address up with cudaGetSymbolAddress on the device it runs on, with that
+// device current (cheap, and it allocates nothing), so a cudaDeviceReset in
+// between cannot leave a stale address behind. Every call runs its kernels on
+// the legacy default stream, reads reduction results back to the host with
+// cudaMemcpy each sweep and ends with cudaDeviceSynchronize: it must not be
+// called while any stream on the device is being captured.
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstring>
-#include <mutex>
 
 #include "common.h"
 #include "device.cuh"
@@ -36,12 +39,8 @@ using excent::ull;
 
 constexpr int NOALLOC_MAX_N = EXCENT_NOALLOC_MAX_N;
 constexpr int NOALLOC_RED = 64;   // reduction slots (doubles) after the two vectors
-constexpr int NOALLOC_MAX_DEVICES = 64;
 
 static __device__ __align__(256) double g_noalloc_scratch[2 * (size_t)NOALLOC_MAX_N + NOALLOC_RED];
-
-std::mutex g_addr_mu;
-double* g_addr[NOALLOC_MAX_DEVICES] = {};
 
 // y[v] = sum over the list of v of x[u]; one warp per vertex.
 __global__ void k_na_spmv(int n, const ull* idx, const int* adj, const double* x, double* y, double c, double s) {
@@ -79,18 +78,14 @@ __global__ void k_na_tofloat(int n, const double* x, float* y) {
         y[v] = (float)x[v];
 }
 
-// Device address of the scratch array on the current device (looked up once).
-int scratch_address(int device, double** out) {
-    if (device < 0 || device >= NOALLOC_MAX_DEVICES) EX_FAIL(EXCENT_ERR_ARG, "device %d out of range", device);
-    std::lock_guard<std::mutex> lk(g_addr_mu);
-    if (!g_addr[device]) {
-        double* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p)
-            EX_FAIL(EXCENT_ERR_CUDA, "cudaGetSymbolAddress of the scratch array failed (%s)", cudaGetErrorString(e));
-        g_addr[device] = p;
-    }
-    *out = g_addr[device];
+// Device address of the scratch array on the current device, looked up on
+// every call (the caller has made the device current).
+int scratch_address(double** out) {
+    double* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+        EX_FAIL(EXCENT_ERR_CUDA, "cudaGetSymbolAddress of the scratch array failed (%s)", cudaGetErrorString(e));
+    *out = p;
     return EXCENT_OK;
 }
 
@@ -116,7 +111,7 @@ extern "C" int excent_params_fp64_noalloc(int device, int n, const unsigned long
                  "use excent_params_fp64", n, NOALLOC_MAX_N);
     EX_CUDA(cudaSetDevice(device));
     double* base = nullptr;
-    EX_TRY(scratch_address(device, &base));
+    EX_TRY(scratch_address(&base));
     double* v0 = base;
     double* v1 = base + NOALLOC_MAX_N;
     double* red = base + 2 * (size_t)NOALLOC_MAX_N;
@@ -131,6 +126,7 @@ extern "C" int excent_params_fp64_noalloc(int device, int n, const unsigned long
     for (; pit < 5000; pit++) {
         k_na_spmv<<<wb, 256>>>(n, d_idx, d_adj, v0, v1, 0.0, 1.0);
         EX_TRY(sums(n, v1, red, G, &ss, nullptr));
+        if (!(ss > 0)) EX_FAIL(EXCENT_ERR_ARG, "params: the graph has no edges (A x = 0), lambda1 is undefined");
         lam = std::sqrt(ss);
         k_na_affine<<<G, 256>>>(n, v1, 1.0 / lam, 0.0);
         std::swap(v0, v1);

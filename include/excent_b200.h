@@ -163,6 +163,15 @@ int excent_engine_hot_setup(excent_engine* e, int nh, const int32_t* ids, const 
  * pending count stays on the device: no host synchronisation per range. */
 int excent_engine_push_hot(excent_engine* e, int lo, int hi, int after_slots);
 
+/* The pending hot vertices among hot ids [lo, hi) on the current residuals,
+ * as indices into the hot id list (unordered), and their count: the
+ * compaction step of excent_engine_push_hot alone, synchronous
+ * (src/excent.cu:178-182, 617-618). */
+int excent_engine_hot_pending(excent_engine* e, int lo, int hi, int32_t* out, unsigned int* k);
+/* Copy the hot cache's edge lists (off[nh] entries) to the host, after the
+ * pass-0 fills of excent_engine_push_stream (src/excent.cu:211-220, 704-705). */
+int excent_engine_hot_edges(excent_engine* e, int32_t* out);
+
 /* Wait for all engine streams. */
 int excent_engine_sync(excent_engine* e);
 
@@ -471,10 +480,13 @@ int excent_params_fp64(int device, int n, const unsigned long long* d_idx, const
  * vectors and reduction slots live in a static device array of the library
  * (16 MiB + 512 bytes, held by every GPU that loads the library until exit),
  * so n must be <= EXCENT_NOALLOC_MAX_N; larger graphs get EXCENT_ERR_ARG.
- * The first call on a device looks the array's address up
- * (cudaGetSymbolAddress) and should come before any stream capture. All
- * calls share the array: calls that overlap on the GPU race and must be
- * serialised by the caller. No counterpart in the reference. */
+ * Each call looks the array's address up (cudaGetSymbolAddress) on the
+ * device it runs on, runs on the legacy default stream, reads sums back to
+ * the host every sweep and ends with cudaDeviceSynchronize, so it must not
+ * be called while any stream on the device is being captured. All calls
+ * share the array: calls that overlap on the GPU race and must be serialised
+ * by the caller. A graph with no edges gets EXCENT_ERR_ARG, as with
+ * excent_params_fp64. No counterpart in the reference. */
 #define EXCENT_NOALLOC_MAX_N (1 << 20)
 int excent_params_fp64_noalloc(int device, int n, const unsigned long long* d_idx, const int32_t* d_adj,
                                double katz_numerator, double* out, float* d_v1);

@@ -29,11 +29,21 @@ _u8p = C.POINTER(C.c_uint8)
 _u16p = C.POINTER(C.c_uint16)
 
 
+def reference_root() -> str:
+    """Where the reference checkout is: $EXCENT_REFERENCE, else the Makefile's REF default."""
+    r = os.environ.get("EXCENT_REFERENCE")
+    if r:
+        return r
+    out = subprocess.run(["make", "-s", "-C", HERE, "print-ref"], capture_output=True, text=True)
+    return out.stdout.strip()
+
+
 def build() -> None:
     """Compile liboracle.so (and the reference harnesses when the reference checkout exists)."""
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
-    if os.path.isdir("/root/reference/src"):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    ref = reference_root()
+    if ref and os.path.isdir(os.path.join(ref, "src")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref}"], check=True)
 
 
 _lib = None

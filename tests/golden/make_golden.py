@@ -21,7 +21,19 @@ import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = "/root/reference/datasets/sample"
+
+
+def reference_root():
+    """The reference checkout: $EXCENT_REFERENCE, else oracle/Makefile's REF default."""
+    r = os.environ.get("EXCENT_REFERENCE")
+    if r:
+        return r
+    out = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "print-ref"], capture_output=True,
+                         text=True)
+    return out.stdout.strip()
+
+
+REF = os.path.join(reference_root(), "datasets", "sample")
 REF_BIN = os.path.join(ROOT, "oracle", "_ref")
 
 

@@ -43,6 +43,38 @@ def test_noalloc_matches_allocating_entry_point_twice(scale, seed):
     g.close()
 
 
+def test_noalloc_call_leaves_free_device_memory_unchanged():
+    """The property the entry point exists for: after a warm-up call (module
+    load, lazy context state), a further call takes no device memory at all."""
+    g = X.DeviceGraph(12, 16, 3)
+    di, da, _ = g.device_ptrs()
+    out = np.zeros(5, dtype=np.float64)
+    v1 = torch.empty(g.n, dtype=torch.float32, device="cuda")
+    call("excent_params_fp64_noalloc", 0, g.n, di, da, 0.85, out.ctypes.data_as(C.POINTER(C.c_double)), v1.data_ptr())
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        call("excent_params_fp64_noalloc", 0, g.n, di, da, 0.85, out.ctypes.data_as(C.POINTER(C.c_double)),
+             v1.data_ptr())
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    g.close()
+
+
+def test_noalloc_rejects_an_edgeless_graph():
+    L = load()
+    n = 64
+    idx = torch.zeros(n + 1, dtype=torch.int64, device="cuda")
+    adj = torch.zeros(1, dtype=torch.int32, device="cuda")
+    out = np.zeros(5, dtype=np.float64)
+    for fn in ("excent_params_fp64_noalloc", "excent_params_fp64"):
+        rc = getattr(L, fn)(0, n, C.c_void_p(idx.data_ptr()), C.c_void_p(adj.data_ptr()), C.c_double(0.85),
+                            out.ctypes.data_as(C.POINTER(C.c_double)), None)
+        assert rc == 1, fn
+        assert b"no edges" in L.excent_last_error()
+
+
 def test_noalloc_rejects_graphs_beyond_its_scratch():
     L = load()
     out = np.zeros(5, dtype=np.float64)
