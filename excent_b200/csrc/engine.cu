@@ -1571,6 +1571,36 @@ extern "C" int excent_engine_push_hot(excent_engine* e, int lo, int hi, int afte
     return EXCENT_OK;
 }
 
+extern "C" int excent_engine_hot_pending(excent_engine* e, int lo, int hi, int32_t* out, unsigned int* k) {
+    EX_CHECK_ARG(e && e->d_hedges && out && k, "no hot cache or null argument");
+    EX_CHECK_ARG(lo >= 0 && lo <= hi && hi <= e->nh, "bad hot range");
+    EX_CUDA(cudaSetDevice(e->dev));
+    EX_CUDA(cudaMemsetAsync(&e->d_ctrl->hcount, 0, sizeof(unsigned), e->s_main));
+    if (hi > lo) {
+        const int grid = (int)std::min<long long>(((long long)(hi - lo) + BLOCK - 1) / BLOCK, (long long)e->sms * 8);
+        if (e->L == 1) k_compact_hot<1><<<grid, BLOCK, 0, e->s_main>>>(lo, hi, e->d_hids, e->d_r, e->M, e->d_hlist, e->d_ctrl);
+        else k_compact_hot<4><<<grid, BLOCK, 0, e->s_main>>>(lo, hi, e->d_hids, e->d_r, e->M, e->d_hlist, e->d_ctrl);
+        e->launches++;
+        EX_CUDA(cudaGetLastError());
+    }
+    unsigned cnt = 0;
+    EX_CUDA(cudaMemcpyAsync(&cnt, &e->d_ctrl->hcount, sizeof(unsigned), cudaMemcpyDeviceToHost, e->s_main));
+    EX_CUDA(cudaStreamSynchronize(e->s_main));
+    *k = cnt;
+    if (cnt) EX_CUDA(cudaMemcpy(out, e->d_hlist, (size_t)cnt * sizeof(int), cudaMemcpyDeviceToHost));
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_hot_edges(excent_engine* e, int32_t* out) {
+    EX_CHECK_ARG(e && e->d_hedges && out, "no hot cache or null argument");
+    EX_CUDA(cudaSetDevice(e->dev));
+    EX_CUDA(cudaDeviceSynchronize());
+    ull he = 0;
+    EX_CUDA(cudaMemcpy(&he, e->d_hoff + e->nh, sizeof(ull), cudaMemcpyDeviceToHost));
+    if (he) EX_CUDA(cudaMemcpy(out, e->d_hedges, he * sizeof(int), cudaMemcpyDeviceToHost));
+    return EXCENT_OK;
+}
+
 extern "C" int excent_engine_sync(excent_engine* e) {
     EX_CHECK_ARG(e, "null engine");
     EX_CUDA(cudaSetDevice(e->dev));

@@ -146,6 +146,92 @@ def test_snapshot_bitexact_vs_oracle_and_reference(rmat12, nm, cap, use_hot):
     eng.close()
 
 
+@pytest.mark.parametrize("nm", [1, 3])
+@pytest.mark.parametrize("cap", [1000, 10 ** 9])
+def test_hot_compact_and_fill_bitexact_vs_reference(rmat12, nm, cap):
+    """The degree cache's integer work on identical inputs: the pending hot
+    list of each chunk's hot range (as a sorted set) against the reference's
+    k_compact_hot, and the pass-0 fill of the hot lists out of streamed chunks
+    against the reference's k_fill_hot and the CSR itself (src/excent.cu:178-182,
+    211-220, 617-618, 704-705)."""
+    import excent_b200._capi as K
+    n, idx, adj = rmat12
+    eps, r, v0, e, _, _ = snapshot_case(nm, 29 + nm, n, idx, cap, 0.05)
+    deg = np.diff(idx.astype(np.int64))
+    # the highest-degree vertices (ties by id), as the degree cache holds them
+    hot_ids = np.sort(np.argsort(-deg, kind="stable")[:max(1, n // 20)]).astype(np.int32)
+    hot_ids = hot_ids[deg[hot_ids] > 0]
+    hot = np.zeros((n + 31) // 32, dtype=np.uint32)
+    for v in hot_ids:
+        hot[v >> 5] |= np.uint32(1 << int(v & 31))
+    hoff = np.zeros(len(hot_ids) + 1, dtype=np.uint64)
+    hoff[1:] = np.cumsum(deg[hot_ids])
+    meas = X.measures("all" if nm == 3 else "pr", alpha=0.1, lam=10.0, eps_katz=1.0, eps_ev=1.0)
+    meas.nm = nm
+    for k in range(nm):
+        meas.eps[k] = float(eps[k])
+    eng = X.Engine(n, len(adj), meas, v0, e)
+    eng.upload_offsets(idx)
+    K.call("excent_engine_hot_setup", eng.h, len(hot_ids), hot_ids.ctypes.data_as(K.i32p),
+           hoff.ctypes.data_as(K.u64p), hot.ctypes.data_as(K.u32p))
+    eng.init()
+    for k in range(nm):
+        eng.write(k, r=r[k])
+    L = ref_kernels()
+    L.ref_compact_hot.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_void_p]
+    L.ref_fill_hot.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p,
+                               C.c_void_p]
+    dev = torch.device("cuda")
+    d_r = [torch.from_numpy(r[k]).to(dev) for k in range(nm)]
+    d_hids = torch.from_numpy(hot_ids).to(dev)
+    d_hoff = torch.from_numpy(hoff.view(np.int64)).to(dev)
+    d_idx = torch.from_numpy(idx.view(np.int64)).to(dev)
+    rp = (C.c_void_p * 3)(*[t.data_ptr() for t in d_r], *([0] * (3 - nm)))
+    ep = (C.c_float * 3)(*[float(x) for x in eps], *([0.0] * (3 - nm)))
+    out = torch.zeros(max(len(hot_ids), 1), dtype=torch.int32, device=dev)
+    count = torch.zeros(1, dtype=torch.int32, device=dev)
+    bounds = list(v0) + [n]
+    ranges = [(int(np.searchsorted(hot_ids, bounds[c])), int(np.searchsorted(hot_ids, bounds[c + 1])))
+              for c in range(len(v0))] + [(0, len(hot_ids))]
+    pend = np.zeros(n, bool)
+    for k in range(nm):
+        pend |= np.abs(r[k]) > eps[k]
+    mine = np.zeros(max(len(hot_ids), 1), dtype=np.int32)
+    for lo, hi in ranges:
+        kk = C.c_uint()
+        K.call("excent_engine_hot_pending", eng.h, lo, hi, mine.ctypes.data_as(K.i32p), C.byref(kk))
+        got = np.sort(mine[:kk.value])
+        assert np.array_equal(got, lo + np.nonzero(pend[hot_ids[lo:hi]])[0]), (lo, hi)
+        assert L.ref_compact_hot(lo, hi, d_hids.data_ptr(), nm, rp, ep, out.data_ptr(), count.data_ptr()) == 0
+        assert np.array_equal(got, np.sort(out[:int(count.item())].cpu().numpy())), (lo, hi)
+    # pass-0 fill: stream every chunk through slot 0 with an empty demand table (no push)
+    K.call("excent_engine_slots_create", eng.h, int(max(np.diff(np.asarray(e, dtype=np.int64)).max(), 1)),
+           int(np.diff(bounds).max()), 0)
+    ed = C.POINTER(C.c_int32)()
+    K.call("excent_engine_slot_buffers", eng.h, 0, C.byref(ed), None, None)
+    zero = np.zeros(2 * len(v0), dtype=np.uint64)
+    d_hedges = torch.zeros(max(int(hoff[-1]), 1), dtype=torch.int32, device=dev)
+    e_all = [int(x) for x in e]   # nc + 1 edge bounds
+    for c in range(len(v0)):
+        lo, hi = ranges[c]
+        ne = int(e_all[c + 1] - e_all[c])
+        K.call("excent_engine_slot_wait", eng.h, 0)
+        np.ctypeslib.as_array(ed, shape=(max(ne, 1),))[:ne] = adj[e_all[c]:e_all[c + 1]]
+        K.call("excent_engine_push_stream", eng.h, 0, c, zero.ctypes.data_as(K.u64p), 0.5, 0, lo, hi)
+        if hi > lo:
+            src = torch.from_numpy(np.ascontiguousarray(adj[e_all[c]:e_all[c + 1]])).to(dev)
+            assert L.ref_fill_hot(lo, hi, d_hids.data_ptr(), d_hoff.data_ptr(), d_idx.data_ptr(), int(e_all[c]),
+                                  src.data_ptr(), d_hedges.data_ptr()) == 0
+    eng.sync()
+    hedges = np.zeros(max(int(hoff[-1]), 1), dtype=np.int32)
+    K.call("excent_engine_hot_edges", eng.h, hedges.ctypes.data_as(K.i32p))
+    want = np.concatenate([adj[idx[v]:idx[v + 1]] for v in hot_ids]) if len(hot_ids) else np.zeros(0, np.int32)
+    assert np.array_equal(hedges[:len(want)], want)
+    assert np.array_equal(d_hedges.cpu().numpy()[:len(want)], want)
+    eng.close()
+
+
 @pytest.mark.parametrize("measure", ["pr", "katz", "ev", "all"])
 def test_init_matches_reference_k_init(sample, measure):
     n, idx, adj, env = sample
