@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--config", default="cached-all", choices=sorted(CONFIGS))
     ap.add_argument("--scale", type=int, default=None, help="override the graph scale (smaller test runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--errors", default="on", choices=["on", "off"],
+                    help="error against the FP64 oracle solution, like-for-like run and the reference engine's error")
     ap.add_argument("--no-graph", action="store_true", help="host-driven pass loop instead of the CUDA graph")
     ap.add_argument("--ev-project", default="on", choices=["on", "off"],
                     help="FP64 eigenvector normalisation step (remove the principal-eigenvector component of the "
@@ -166,6 +168,105 @@ def push_bytes(nm, log):
     ep = sum(int(l.pushed) for l in log)
     pv = sum(int(l.pending) for l in log)
     return 4 * ep + 8 * nm * ep + pv * (16 + 16 * nm), ep, pv
+
+
+def top_k(v, k):
+    """Indices of the k largest entries of v, ties broken by the lower index."""
+    k = min(k, len(v))
+    if k == 0:
+        return np.zeros(0, dtype=np.int64)
+    kth = np.partition(v, len(v) - k)[len(v) - k]
+    cand = np.nonzero(v >= kth)[0]
+    return cand[np.lexsort((cand, -v[cand]))[:k]]
+
+
+def unit_signed(v):
+    """Unit L2 norm with the sign fixed by the sum, as the reference's comparison tool treats
+    eigenvectors (tools/centrality_reference.cu:71-76)."""
+    v = np.asarray(v, dtype=np.float64)
+    s, t = float(np.dot(v, v)), float(v.sum())
+    return v * ((-1.0 if t < 0 else 1.0) / np.sqrt(s)) if s > 0 else v
+
+
+def error_vs_fp64(measure, ref, x):
+    """L1 error relative to the FP64 solution's mass, max per-vertex error and top-1000 overlap."""
+    r = np.asarray(ref, dtype=np.float64)
+    xx = np.asarray(x, dtype=np.float32).astype(np.float64)
+    if measure == "ev":
+        r, xx = unit_signed(r), unit_signed(xx)
+    d = np.abs(xx - r)
+    return {"l1_rel": float(d.sum() / np.abs(r).sum()), "max_abs": float(d.max()),
+            "top1000": int(len(np.intersect1d(top_k(r, 1000), top_k(xx, 1000))))}
+
+
+def fp64_solutions(n, d_idx, d_adj, kinds, alpha, device):
+    """FP64 Jacobi / power-iteration solutions on the device (tol 1e-9, as the reference's oracle)."""
+    import excent_b200 as X
+    out = {}
+    for k in kinds:
+        t0 = time.perf_counter()
+        out[k], it = X.reference_fp64(n, d_idx, d_adj, k, alpha=alpha if k == "katz" else 0.0, beta=1.0, tol=1e-9,
+                                      device=device)
+        log(f"FP64 {k}: {it} iterations, {time.perf_counter() - t0:.1f}s")
+    return out
+
+
+def error_report(a, n, m, d_idx, d_adj, idx_np, adj_np, v0, e, eng, meas, measure, lam, device):
+    """Error of this engine's results against the FP64 oracle solution, in the timed configuration and
+    like for like with the reference engine (eigenvector initial residual from lambda1 rounded to float,
+    no FP64 eigenvector step, the same pass cap), beside the reference engine's own error: its CLI
+    (src/excent.cu built from source) on the same EGR file and constants, results through --dump
+    (src/excent.cu:763-777)."""
+    import shutil
+
+    import excent_b200 as X
+    kinds = ["pr", "katz", "ev"] if measure == "all" else [measure]
+    alpha = 0.9 / lam if lam else None
+    ref = fp64_solutions(n, d_idx, d_adj, kinds, alpha, device)
+    rep = {"oracle": "FP64 Jacobi (PageRank, Katz) and power iteration (eigenvector) on the device to a relative "
+                     "change of 1e-9 (tools/centrality_reference.cu:184-214); the eigenvector is compared as a "
+                     "unit vector with its sign fixed by its sum",
+           "timed_config": {k: error_vs_fp64(k, ref[k], eng.read(i)) for i, k in enumerate(kinds)}}
+    if measure == "all":
+        meas_l = X.measures("all", alpha=alpha, beta=1.0, lam=lam, eps_pr=1e-2, eps_katz=1e-6, eps_ev=1e-6,
+                            ev_init_fp64=False)
+        eng2 = X.Engine(n, m, meas_l, v0, e, device=device)
+        eng2.upload_device(d_idx, d_adj)
+        eng2.set_hub_targets(min(4096, n))
+        eng2.set_hub_order(a.hub_order)
+        st = eng2.solve(list_frac=a.list_frac, max_passes=a.ref_passes)
+        rep["like_for_like"] = {"ev_init": "lambda1 rounded to float", "ev_project": "off",
+                                "max_passes": a.ref_passes, "passes": st.passes,
+                                **{k: error_vs_fp64(k, ref[k], eng2.read(i)) for i, k in enumerate(kinds)}}
+        eng2.close()
+    ref_bin = os.path.join(ROOT, "oracle", "_ref", "excent")
+    if not os.path.exists(ref_bin):
+        rep["reference_engine"] = {"unavailable": "reference CLI not built (oracle/Makefile)"}
+        return rep
+    d = tempfile.mkdtemp(prefix="excent_err_")
+    try:
+        path = os.path.join(d, "g.egr")
+        X.write_egr(path, idx_np, adj_np)
+        args = [path, "--measure", measure, "--cache", "chunks", "--stream-ratio", "2", "--dump",
+                os.path.join(d, "out"), "--max-passes", str(a.ref_passes)]
+        if measure == "all":
+            args += ["--alpha", "%.9g" % alpha, "--beta", "1", "--lambda", "%.17g" % lam, "--eps-katz", "1e-6",
+                     "--eps-ev", "1e-6"]
+        r = subprocess.run([ref_bin, *args], capture_output=True, text=True, timeout=1800,
+                           env=dict(os.environ, HOME=d))
+        if r.returncode != 0:
+            rep["reference_engine"] = {"error": (r.stderr or r.stdout)[-300:]}
+            return rep
+        import re
+        mp = re.search(r"^passes (\d+)", r.stdout, re.M)
+        got = {"args": " ".join(args[1:]).replace(d, "<tmp>"), "passes": int(mp.group(1)) if mp else None}
+        for k in kinds:
+            x = np.fromfile(os.path.join(d, f"out.{k}.bin"), dtype=np.float32)
+            got[k] = error_vs_fp64(k, ref[k], x)
+        rep["reference_engine"] = got
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    return rep
 
 
 def run_ours(a, world, rank, local, dist):
@@ -312,6 +413,10 @@ def run_ours(a, world, rank, local, dist):
         "gpu_launches": int(launches),
     }
     log(f"profiled solve: {prof}")
+    if rank == 0 and world == 1 and a.errors == "on":
+        result["error_vs_fp64"] = error_report(a, n, m, d_idx, d_adj, idx_np, h_adj.numpy()[:m], v0, e, eng, meas,
+                                               measure, lam, local)
+        log(f"error vs FP64: {json.dumps(result['error_vs_fp64'])}")
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(n, idx_np, h_adj.numpy()[:m], meas, measure, lam)
     if rank == 0 and world == 1 and a.ref_gpu:

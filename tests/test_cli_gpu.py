@@ -116,6 +116,41 @@ def test_cli_sample_matches_reference_binary(tmp_path):
             assert ca["l1_rel"] <= cb["l1_rel"] * 1.05, (k, ca, cb)
 
 
+@pytest.fixture(scope="module")
+def rmat16_cfg(tmp_path_factory):
+    """The reference's CPU-runnable configuration: R-MAT scale 16, edge factor 16, seed 1,
+    symmetric, written as wide EGR, with its given constants (tools/excent_params.cu rules)."""
+    d = tmp_path_factory.mktemp("cfg1")
+    n, idx, adj = O.rmat_graph(16, 16, 1)
+    p = str(d / "r16.egr")
+    O.write_egr(p, idx, adj, wide=True)
+    par = O.params(n, idx, adj)
+    env = {k: par[k] for k in ("LAMBDA", "ALPHA", "BETA", "EPS_PR", "EPS_KATZ", "EPS_EV")}
+    return p, n, idx, adj, env
+
+
+@pytest.mark.parametrize("measure", ["pr", "all"])
+@pytest.mark.parametrize("mode", ["host", "device-loop"])
+def test_error_no_looser_than_reference_binary_rmat16(rmat16_cfg, tmp_path, measure, mode):
+    """Error against the FP64 oracle (L1 relative, max per-vertex, top-1000 overlap) of this
+    repo's CLI against the reference binary's on the same R-MAT scale-16 file and flags.
+    Both are FP32 with atomics in a run-dependent order; the allowance for that is 5 % of
+    L1, 25 % of the max per-vertex error and 5 of the top 1000."""
+    if not os.path.exists(REF_CLI):
+        pytest.skip("reference binary not built")
+    p, n, idx, adj, env = rmat16_cfg
+    args = [p, *env_args(env, measure), "--stream-ratio", "2", "--cache", "chunks"]
+    run(CLI, args + (["--device-loop"] if mode == "device-loop" else []) + ["--dump", str(tmp_path / "a")], tmp_path)
+    run(REF_CLI, args + ["--dump", str(tmp_path / "b")], tmp_path)
+    for k in (["pr", "katz", "ev"] if measure == "all" else ["pr"]):
+        ref_x = O.reference_solution(n, idx, adj, k, alpha=float(env["ALPHA"]))
+        a = O.compare(k, ref_x, np.fromfile(str(tmp_path / f"a.{k}.bin"), dtype=np.float32))
+        b = O.compare(k, ref_x, np.fromfile(str(tmp_path / f"b.{k}.bin"), dtype=np.float32))
+        assert a["l1_rel"] <= 1.05 * b["l1_rel"] + 1e-7, (k, a, b)
+        assert a["max_abs"] <= 1.25 * b["max_abs"] + 1e-7, (k, a, b)
+        assert a["top1000"] >= b["top1000"] - 5, (k, a, b)
+
+
 def test_cli_trace_and_hot_rank_roundtrip(rmat14, tmp_path):
     """--trace-pending writes uint16 pass counts; they drive --hot-rank."""
     p, n, idx, adj, env = rmat14
