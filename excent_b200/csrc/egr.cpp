@@ -1,4 +1,4 @@
-// egr.cpp -- EgrFile (egr.h) and its C entry points.
+// egr.cpp -- GraphFile (egr.h) and the excent_egr_* C entry points.
 #include "egr.h"
 
 #include <fcntl.h>
@@ -16,161 +16,208 @@
 
 namespace excent {
 
-EgrFile::~EgrFile() {
-    if (map_ && map_ != MAP_FAILED) munmap(map_, map_size_);
+namespace {
+
+constexpr size_t kPiece = size_t(8) << 20;   // bytes per positional read of a bulk range
+
+// What the first bytes of an EGR file say, before anything is mapped.
+struct Header {
+    int32_t n = 0;
+    ull m = 0;
+    bool wide = false;
+    size_t offsets_at = 0, entries_at = 0;
+};
+
+size_t page_bytes() { return (size_t)sysconf(_SC_PAGESIZE); }
+
+}  // namespace
+
+GraphFile::~GraphFile() {
+    if (map_.base) munmap(map_.base, map_.bytes);
     if (fd_ >= 0) ::close(fd_);
 }
 
-int EgrFile::read_exact(void* dst, size_t bytes, size_t off) const {
-    char* p = (char*)dst;
-    while (bytes) {
-        const ssize_t r = pread(fd_, p, bytes, (off_t)off);
-        if (r < 0 && errno == EINTR) continue;
-        if (r <= 0) return EXCENT_ERR_IO;
-        p += r;
-        off += (size_t)r;
-        bytes -= (size_t)r;
+// One positional read of exactly `bytes` (retried on short reads and EINTR).
+int GraphFile::pread_all(void* dst, size_t bytes, size_t at) const {
+    char* out = static_cast<char*>(dst);
+    size_t done = 0;
+    while (done < bytes) {
+        const ssize_t got = pread(fd_, out + done, bytes - done, (off_t)(at + done));
+        if (got < 0 && errno == EINTR) continue;
+        if (got <= 0) return EXCENT_ERR_IO;
+        done += (size_t)got;
     }
     return EXCENT_OK;
 }
 
-// 8 MiB pieces over up to io_threads threads (include/StaticGraph.h:160-170).
-int EgrFile::read_parallel(void* dst, size_t bytes, size_t off) const {
-    const size_t piece = 8ull << 20;
-    const long long pieces = (long long)((bytes + piece - 1) / piece);
-    const int threads = (int)std::min<long long>(io_threads_, std::max<long long>(1, pieces));
-    std::atomic<int> bad{0};
-#pragma omp parallel for num_threads(threads) schedule(static, 1)
-    for (long long i = 0; i < pieces; i++) {
-        const size_t b = (size_t)i * piece;
-        if (read_exact((char*)dst + b, std::min(piece, bytes - b), off + b) != EXCENT_OK) bad = 1;
+// A bulk range: the reader team claims 8 MiB pieces from a shared cursor
+// until none is left, so a slow piece does not hold back a fixed share.
+int GraphFile::pread_team(void* dst, size_t bytes, size_t at) const {
+    if (bytes == 0) return EXCENT_OK;
+    const size_t pieces = (bytes + kPiece - 1) / kPiece;
+    const int team = (int)std::min<size_t>((size_t)team_, pieces);
+    std::atomic<size_t> cursor{0};
+    std::atomic<bool> failed{false};
+#pragma omp parallel num_threads(team)
+    {
+        for (size_t p = cursor.fetch_add(1); p < pieces && !failed.load(std::memory_order_relaxed);
+             p = cursor.fetch_add(1)) {
+            const size_t b = p * kPiece, len = std::min(kPiece, bytes - b);
+            if (pread_all(static_cast<char*>(dst) + b, len, at + b) != EXCENT_OK) failed = true;
+        }
     }
-    return bad ? EXCENT_ERR_IO : EXCENT_OK;
+    return failed ? EXCENT_ERR_IO : EXCENT_OK;
 }
 
-int EgrFile::open(const char* path, int io_threads, bool offsets_in_ram, bool validate) {
-    io_threads_ = std::max(1, io_threads);
+int GraphFile::open(const char* path, int io_threads, bool offsets_in_ram, bool check_offsets) {
+    team_ = std::max(1, io_threads);
     fd_ = ::open(path, O_RDONLY);
     if (fd_ < 0) EX_FAIL(EXCENT_ERR_IO, "%s: %s", path, strerror(errno));
     struct stat st;
     if (fstat(fd_, &st) != 0) EX_FAIL(EXCENT_ERR_IO, "%s: %s", path, strerror(errno));
-    const size_t fsize = (size_t)st.st_size;
-    int32_t hdr[2];
-    if (fsize < sizeof hdr || read_exact(hdr, sizeof hdr, 0) != EXCENT_OK)
+    const size_t file_bytes = (size_t)st.st_size;
+
+    // header: 8 bytes, 16 for the wide form
+    Header h;
+    int32_t head[2] = {0, 0};
+    if (file_bytes < sizeof head || pread_all(head, sizeof head, 0) != EXCENT_OK)
         EX_FAIL(EXCENT_ERR_IO, "%s: short header", path);
-    n = hdr[0];
-    size_t off = sizeof hdr;
-    wide = hdr[1] == -1;
-    if (wide) {
-        int64_t mm = 0;
-        if (read_exact(&mm, sizeof mm, off) != EXCENT_OK) EX_FAIL(EXCENT_ERR_IO, "%s: short header", path);
-        if (mm < 0) EX_FAIL(EXCENT_ERR_IO, "%s: bad header (negative edge count)", path);
-        m = (ull)mm;
-        off += sizeof mm;
+    h.n = head[0];
+    h.wide = head[1] == -1;
+    if (h.wide) {
+        int64_t m64 = -1;
+        if (file_bytes < 16 || pread_all(&m64, sizeof m64, sizeof head) != EXCENT_OK)
+            EX_FAIL(EXCENT_ERR_IO, "%s: short header", path);
+        if (m64 < 0) EX_FAIL(EXCENT_ERR_IO, "%s: bad header (negative edge count)", path);
+        h.m = (ull)m64;
+        h.offsets_at = 16;
     } else {
-        if (hdr[1] < 0) EX_FAIL(EXCENT_ERR_IO, "%s: bad header (edge count %d)", path, hdr[1]);
-        m = (ull)hdr[1];
+        if (head[1] < 0) EX_FAIL(EXCENT_ERR_IO, "%s: bad header (edge count %d)", path, head[1]);
+        h.m = (ull)head[1];
+        h.offsets_at = 8;
     }
-    if (n < 1) EX_FAIL(EXCENT_ERR_IO, "StaticGraph: bad header in %s", path);
-    idx_off_ = off;
-    const size_t ib = ((size_t)n + 1) * (wide ? sizeof(ull) : sizeof(int32_t));
-    nlist_off_ = off + ib;
-    if (fsize < nlist_off_ + m * sizeof(int32_t))
-        EX_FAIL(EXCENT_ERR_IO, "%s: truncated (%zu bytes, header needs %llu)", path, fsize,
-                (ull)(nlist_off_ + m * sizeof(int32_t)));
-    if (!wide) offsets_in_ram = true;
-    if (offsets_in_ram) {
-        ram_off_.resize((size_t)n + 1);
-        if (wide) {
-            if (read_parallel(ram_off_.data(), ib, off) != EXCENT_OK) EX_FAIL(EXCENT_ERR_IO, "%s: pread of offsets failed", path);
-        } else {
-            std::vector<uint32_t> tmp((size_t)n + 1);
-            if (read_parallel(tmp.data(), ib, off) != EXCENT_OK) EX_FAIL(EXCENT_ERR_IO, "%s: pread of offsets failed", path);
-            for (size_t i = 0; i < tmp.size(); i++) ram_off_[i] = tmp[i];
-        }
+    if (h.n < 1) EX_FAIL(EXCENT_ERR_IO, "StaticGraph: bad header in %s", path);
+    const size_t offset_width = h.wide ? sizeof(ull) : sizeof(uint32_t);
+    const size_t offsets_bytes = ((size_t)h.n + 1) * offset_width;
+    h.entries_at = h.offsets_at + offsets_bytes;
+    const size_t need = h.entries_at + h.m * sizeof(int32_t);
+    if (file_bytes < need)
+        EX_FAIL(EXCENT_ERR_IO, "%s: truncated (%zu bytes, header needs %llu)", path, file_bytes, (ull)need);
+    n = h.n;
+    m = h.m;
+    wide = h.wide;
+    offsets_at_ = h.offsets_at;
+    entries_at_ = h.entries_at;
+
+    // offsets into RAM: narrow ones widened, wide ones when asked
+    if (!wide) {
+        std::vector<uint32_t> narrow((size_t)n + 1);
+        if (pread_team(narrow.data(), offsets_bytes, offsets_at_) != EXCENT_OK)
+            EX_FAIL(EXCENT_ERR_IO, "%s: pread of offsets failed", path);
+        ram_offsets_.assign(narrow.begin(), narrow.end());
+    } else if (offsets_in_ram) {
+        ram_offsets_.resize((size_t)n + 1);
+        if (pread_team(ram_offsets_.data(), offsets_bytes, offsets_at_) != EXCENT_OK)
+            EX_FAIL(EXCENT_ERR_IO, "%s: pread of offsets failed", path);
     }
-    map_size_ = fsize;
-    map_ = mmap(nullptr, map_size_, PROT_READ, MAP_SHARED, fd_, 0);
-    if (map_ == MAP_FAILED) { map_ = nullptr; EX_FAIL(EXCENT_ERR_IO, "mmap %s: %s", path, strerror(errno)); }
-    madvise(map_, map_size_, MADV_RANDOM);
+
+    void* base = mmap(nullptr, file_bytes, PROT_READ, MAP_SHARED, fd_, 0);
+    if (base == MAP_FAILED) EX_FAIL(EXCENT_ERR_IO, "mmap %s: %s", path, strerror(errno));
+    map_.base = base;
+    map_.bytes = file_bytes;
+    // lists are touched in demand order: no kernel readahead on faults; the
+    // bulk preads still stream sequentially
+    madvise(base, file_bytes, MADV_RANDOM);
     posix_fadvise(fd_, 0, 0, POSIX_FADV_SEQUENTIAL);
-    nlist_ = (const int32_t*)((const char*)map_ + nlist_off_);
-    off_ = offsets_in_ram ? ram_off_.data() : (const ull*)((const char*)map_ + idx_off_);
-    if (validate) {
+    const char* bytes = static_cast<const char*>(base);
+    entries_ = reinterpret_cast<const int32_t*>(bytes + entries_at_);
+    off_ = ram_offsets_.empty() ? reinterpret_cast<const ull*>(bytes + offsets_at_) : ram_offsets_.data();
+
+    if (check_offsets) {
         if (off_[0] != 0 || off_[n] != m) EX_FAIL(EXCENT_ERR_IO, "%s: offsets do not span [0, m]", path);
-        std::atomic<long long> bad{-1};
-#pragma omp parallel for num_threads(io_threads_) schedule(static)
-        for (long long v = 0; v < n; v++)
-            if (off_[v] > off_[v + 1]) bad = v;
-        if (bad >= 0) EX_FAIL(EXCENT_ERR_IO, "%s: offsets decrease at vertex %lld", path, (long long)bad);
+        long long first_bad = -1;
+#pragma omp parallel num_threads(team_)
+        {
+            long long mine = -1;
+#pragma omp for schedule(static) nowait
+            for (long long v = 0; v < n; v++)
+                if (mine < 0 && off_[v] > off_[v + 1]) mine = v;
+#pragma omp critical
+            if (mine >= 0 && (first_bad < 0 || mine < first_bad)) first_bad = mine;
+        }
+        if (first_bad >= 0) EX_FAIL(EXCENT_ERR_IO, "%s: offsets decrease at vertex %lld", path, first_bad);
     }
     return EXCENT_OK;
 }
 
-int EgrFile::read_offsets(size_t v0, size_t cnt, ull* dst) const {
-    if (v0 + cnt > (size_t)n + 1) EX_FAIL(EXCENT_ERR_ARG, "offsets out of range");
-    if (!ram_off_.empty()) { memcpy(dst, ram_off_.data() + v0, cnt * sizeof(ull)); return EXCENT_OK; }
-    if (read_parallel(dst, cnt * sizeof(ull), idx_off_ + v0 * sizeof(ull)) != EXCENT_OK)
+int GraphFile::fetch_offsets(size_t v0, size_t count, ull* dst) const {
+    if (v0 + count > (size_t)n + 1) EX_FAIL(EXCENT_ERR_ARG, "offsets out of range");
+    if (!ram_offsets_.empty()) {
+        std::copy(ram_offsets_.begin() + v0, ram_offsets_.begin() + v0 + count, dst);
+        return EXCENT_OK;
+    }
+    if (pread_team(dst, count * sizeof(ull), offsets_at_ + v0 * sizeof(ull)) != EXCENT_OK)
         EX_FAIL(EXCENT_ERR_IO, "pread of offsets failed");
     return EXCENT_OK;
 }
 
-int EgrFile::read_edges(ull e0, ull e1, int32_t* dst) const {
+int GraphFile::fetch_entries(ull e0, ull e1, int32_t* dst) const {
     if (e0 > e1 || e1 > m) EX_FAIL(EXCENT_ERR_ARG, "edge range out of bounds");
-    if (read_parallel(dst, (e1 - e0) * sizeof(int32_t), nlist_off_ + e0 * sizeof(int32_t)) != EXCENT_OK)
+    if (pread_team(dst, (e1 - e0) * sizeof(int32_t), entries_at_ + e0 * sizeof(int32_t)) != EXCENT_OK)
         EX_FAIL(EXCENT_ERR_IO, "pread of edges [%llu, %llu) failed", e0, e1);
     return EXCENT_OK;
 }
 
-// Merge each part's page runs and request them once (include/StaticGraph.h:90-114).
-void EgrFile::prefetch_lists(const int32_t* vids, int k, ull* pages, ull* runs) const {
-    const size_t P = (size_t)sysconf(_SC_PAGESIZE);
-    ull np = 0, nr = 0;
-    const int parts = std::max(1, std::min(io_threads_, k / 1024));
-#pragma omp parallel for num_threads(parts) reduction(+ : np, nr) schedule(static, 1)
+void GraphFile::readahead_lists(const int32_t* vids, int k, ull* pages, ull* runs) const {
+    const size_t page = page_bytes();
+    const int parts = std::max(1, std::min(team_, k / 1024));
+    std::vector<ull> part_pages(parts, 0), part_runs(parts, 0);
+#pragma omp parallel for num_threads(parts) schedule(static, 1)
     for (int t = 0; t < parts; t++) {
-        const int i0 = (int)((long long)k * t / parts), i1 = (int)((long long)k * (t + 1) / parts);
-        size_t r0 = 0, r1 = 0;
-        bool open = false;
-        auto flush = [&]() {
-            if (!open) return;
-            madvise((char*)map_ + r0 * P, (r1 - r0) * P, MADV_WILLNEED);
-            np += r1 - r0;
-            nr++;
-        };
-        for (int i = i0; i < i1; i++) {
-            const ull d = degree(vids[i]);
-            if (!d) continue;
-            const size_t b0 = nlist_off_ + off_[vids[i]] * sizeof(int32_t), b1 = b0 + d * sizeof(int32_t);
-            const size_t p0 = b0 / P, p1 = (b1 + P - 1) / P;
-            if (open && p0 <= r1) r1 = std::max(r1, p1);
-            else { flush(); r0 = p0; r1 = p1; open = true; }
+        const int lo = (int)((long long)k * t / parts), hi = (int)((long long)k * (t + 1) / parts);
+        // page runs of this part, in list order: [first page, end page)
+        std::vector<std::pair<size_t, size_t>> run;
+        for (int i = lo; i < hi; i++) {
+            const int v = vids[i];
+            const ull len = degree(v);
+            if (len == 0) continue;
+            const size_t b0 = entries_at_ + off_[v] * sizeof(int32_t);
+            const size_t first = b0 / page, end = (b0 + len * sizeof(int32_t) + page - 1) / page;
+            if (!run.empty() && first <= run.back().second) run.back().second = std::max(run.back().second, end);
+            else run.emplace_back(first, end);
         }
-        flush();
+        for (const auto& r : run) {
+            madvise(static_cast<char*>(map_.base) + r.first * page, (r.second - r.first) * page, MADV_WILLNEED);
+            part_pages[t] += r.second - r.first;
+        }
+        part_runs[t] = run.size();
     }
+    ull np = 0, nr = 0;
+    for (int t = 0; t < parts; t++) { np += part_pages[t]; nr += part_runs[t]; }
     *pages = np;
     *runs = nr;
 }
 
-// Unmap our pages and drop them from the page cache (include/StaticGraph.h:116-126).
-void EgrFile::drop_cache(ull e0, ull e1, size_t v0, size_t v1) const {
-    const size_t P = (size_t)sysconf(_SC_PAGESIZE);
-    auto drop = [&](size_t b0, size_t b1) {
-        const size_t a0 = b0 / P * P, a1 = std::min(map_size_, (b1 + P - 1) / P * P);
-        if (a1 <= a0) return;
-        madvise((char*)map_ + a0, a1 - a0, MADV_DONTNEED);
-        posix_fadvise(fd_, (off_t)a0, (off_t)(a1 - a0), POSIX_FADV_DONTNEED);
-    };
-    drop(nlist_off_ + e0 * sizeof(int32_t), nlist_off_ + e1 * sizeof(int32_t));
-    const size_t w = wide ? sizeof(ull) : sizeof(int32_t);
-    drop(idx_off_ + v0 * w, idx_off_ + (v1 + 1) * w);
+// Page-aligned [b0, b1) of the file out of the mapping and the page cache.
+void GraphFile::drop_bytes(size_t b0, size_t b1) const {
+    const size_t page = page_bytes();
+    const size_t lo = b0 - b0 % page, hi = std::min(map_.bytes, (b1 + page - 1) / page * page);
+    if (hi <= lo) return;
+    madvise(static_cast<char*>(map_.base) + lo, hi - lo, MADV_DONTNEED);   // or fadvise keeps our pages
+    posix_fadvise(fd_, (off_t)lo, (off_t)(hi - lo), POSIX_FADV_DONTNEED);
+}
+
+void GraphFile::evict(ull e0, ull e1, size_t v0, size_t v1) const {
+    drop_bytes(entries_at_ + e0 * sizeof(int32_t), entries_at_ + e1 * sizeof(int32_t));
+    const size_t w = wide ? sizeof(ull) : sizeof(uint32_t);
+    drop_bytes(offsets_at_ + v0 * w, offsets_at_ + (v1 + 1) * w);
 }
 
 }  // namespace excent
 
 using namespace excent;
 
-struct excent_egr { EgrFile f; };
+struct excent_egr { GraphFile f; };
 
 extern "C" int excent_egr_open(const char* path, int io_threads, int offsets_in_ram, excent_egr** out) {
     EX_CHECK_ARG(path && out, "null argument");
@@ -192,22 +239,22 @@ extern "C" int excent_egr_info(excent_egr* g, int* n, unsigned long long* m, int
 extern "C" int excent_egr_read_offsets(excent_egr* g, unsigned long long v0, unsigned long long count,
                                        unsigned long long* dst) {
     EX_CHECK_ARG(g && dst, "null argument");
-    return g->f.read_offsets(v0, count, dst);
+    return g->f.fetch_offsets(v0, count, dst);
 }
 extern "C" int excent_egr_read_edges(excent_egr* g, unsigned long long e0, unsigned long long e1, int32_t* dst) {
     EX_CHECK_ARG(g && (dst || e0 == e1), "null argument");
-    return g->f.read_edges(e0, e1, dst);
+    return g->f.fetch_entries(e0, e1, dst);
 }
 extern "C" int excent_egr_prefetch(excent_egr* g, const int32_t* vids, int k, unsigned long long* pages,
                                    unsigned long long* runs) {
     EX_CHECK_ARG(g && pages && runs && (vids || k == 0), "null argument");
     for (int i = 0; i < k; i++) EX_CHECK_ARG(vids[i] >= 0 && vids[i] < g->f.n, "vertex %d out of range", vids[i]);
-    g->f.prefetch_lists(vids, k, pages, runs);
+    g->f.readahead_lists(vids, k, pages, runs);
     return EXCENT_OK;
 }
 extern "C" int excent_egr_drop_cache(excent_egr* g, unsigned long long e0, unsigned long long e1,
                                      unsigned long long v0, unsigned long long v1) {
     EX_CHECK_ARG(g && e0 <= e1 && e1 <= g->f.m && v0 <= v1 && v1 <= (ull)g->f.n, "bad range");
-    g->f.drop_cache(e0, e1, v0, v1);
+    g->f.evict(e0, e1, v0, v1);
     return EXCENT_OK;
 }

@@ -28,15 +28,15 @@ uint64_t splitmix(uint64_t& s) {
 
 // Sampled symmetry check (tools/excent_params.cu:106-118): for random entries
 // e = (v -> u), u's sorted list must hold v. Returns the number of misses.
-int symmetry_misses(const EgrFile& g, int samples) {
+int symmetry_misses(const GraphFile& g, int samples) {
     uint64_t s = 42;
     const ull* off = g.offsets();
     int bad = 0;
     for (int i = 0; i < samples; i++) {
         const ull e = splitmix(s) % g.m;
         const int v = (int)(std::upper_bound(off, off + (size_t)g.n + 1, e) - off) - 1;
-        const int u = g.edges(0)[e];
-        const int32_t* b = g.edges(u);
+        const int u = g.list(0)[e];
+        const int32_t* b = g.list(u);
         const int32_t* en = b + g.degree(u);
         const bool sorted = std::is_sorted(b, en);
         const bool found = sorted ? std::binary_search(b, en, v) : std::find(b, en, v) != en;
@@ -61,7 +61,7 @@ extern "C" int excent_params_main(int argc, char** argv) {
         else { fprintf(stderr, "unknown option %s\n", argv[i]); return 1; }
     }
     const auto t0 = std::chrono::steady_clock::now();
-    EgrFile g;
+    GraphFile g;
     if (g.open(argv[1], 16, true, true) != EXCENT_OK) { fprintf(stderr, "%s: %s\n", argv[1], excent_last_error()); return 1; }
     const int n = g.n;
     const ull m = g.m;
@@ -93,7 +93,7 @@ extern "C" int excent_params_main(int argc, char** argv) {
         const ull piece = ((size_t)1 << 28) / sizeof(int32_t);
         for (ull e0 = 0; e0 < m && !rc; e0 += piece) {
             const ull e1 = std::min(m, e0 + piece);
-            if (g.read_edges(e0, e1, stage) != EXCENT_OK ||
+            if (g.fetch_entries(e0, e1, stage) != EXCENT_OK ||
                 cudaMemcpy(d_adj + e0, stage, (e1 - e0) * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess)
                 rc = 1;
         }

@@ -142,7 +142,7 @@ int solve_mode(int argc, char** argv) {
     const int kind = measure == "pr" ? 0 : measure == "katz" ? 1 : measure == "ev" ? 2 : -1;
     if (kind < 0) { fprintf(stderr, "measure must be pr, katz or ev\n"); return 1; }
     if (kind == 1 && alpha <= 0) { fprintf(stderr, "katz needs --alpha\n"); return 1; }
-    EgrFile g;
+    GraphFile g;
     if (g.open(argv[1], 16, true, true) != EXCENT_OK) { fprintf(stderr, "%s: %s\n", argv[1], excent_last_error()); return 1; }
     const int n = g.n;
     const ull m = g.m;
@@ -163,7 +163,7 @@ int solve_mode(int argc, char** argv) {
         stage.resize((size_t)std::min<ull>(piece, std::max<ull>(m, 1)));
         for (ull e0 = 0; e0 < m && !rc; e0 += piece) {
             const ull e1 = std::min(m, e0 + piece);
-            if (g.read_edges(e0, e1, stage.data()) != EXCENT_OK ||
+            if (g.fetch_entries(e0, e1, stage.data()) != EXCENT_OK ||
                 cudaMemcpy(d_adj + e0, stage.data(), (e1 - e0) * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess)
                 rc = 1;
         }

@@ -213,6 +213,36 @@ def test_hot_select_vs_oracle(rmat14_files, budget):
     assert np.array_equal(np.nonzero(inbits)[0], ido)
 
 
+def test_hot_select_big_degrees_and_ties_vs_oracle():
+    """Degree values of 2^20 and more are admitted whole or not at all, smaller
+    ones partly (the first in id order); synthetic offsets with repeated big and
+    small degrees, budgets at and around every admission boundary."""
+    rng = np.random.default_rng(9)
+    n = 3000
+    deg = rng.integers(0, 40, n).astype(np.uint64)
+    deg[rng.choice(n, 30, replace=False)] = rng.choice([300, 301, 5000], 30)
+    big = rng.choice(n, 9, replace=False)
+    deg[big] = np.array([1 << 20, 1 << 20, (1 << 20) + 7, 3 << 20, 3 << 20, 3 << 20, (1 << 21) - 1, 1 << 21, 5 << 21],
+                        dtype=np.uint64)
+    idx = np.zeros(n + 1, dtype=np.uint64)
+    idx[1:] = np.cumsum(deg)
+    cost = np.sort(deg[deg > 0] * 4 + 16)[::-1].astype(np.int64)
+    marks = np.cumsum(cost)
+    budgets = {0, 15, 16, 17, int(marks[-1]), int(marks[-1]) + 1, 10 ** 13}
+    for i in list(range(0, 12)) + list(range(12, len(marks), 97)):
+        budgets |= {int(marks[i]) - 1, int(marks[i]), int(marks[i]) + 1, int(marks[i]) + 8 * 4 + 16}
+    for budget in sorted(budgets):
+        nh = C.c_int()
+        ids = np.zeros(n, dtype=np.int32)
+        hoff = np.zeros(n + 1, dtype=np.uint64)
+        T = C.c_uint64()
+        K.call("excent_hot_select", n, idx.ctypes.data, budget, None, C.byref(nh), ids.ctypes.data,
+               hoff.ctypes.data, None, C.byref(T))
+        ido, To, Eo = O.hot_select(idx, budget)
+        assert np.array_equal(ids[:nh.value], ido), budget
+        assert T.value == To and hoff[nh.value] == Eo, (budget, T.value, To)
+
+
 def test_hot_select_by_score(rmat14_files):
     """--hot-rank: uint16 scores (the --trace-pending format), boundary score partly taken."""
     n, idx, adj, *_ = rmat14_files
