@@ -66,6 +66,8 @@ PROTOS = [
     ("excent_engine_push_hot", C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
     ("excent_engine_hot_pending", C.c_int, [vp, C.c_int, C.c_int, i32p, C.POINTER(C.c_uint)]),
     ("excent_engine_hot_edges", C.c_int, [vp, i32p]),
+    ("excent_mtx_to_egr", C.c_int, [C.c_char_p, C.c_char_p, C.c_int, u64p]),
+    ("excent_egr_report", C.c_int, [C.c_char_p, C.c_char_p, C.c_int]),
     ("excent_engine_sync", C.c_int, [vp]),
     ("excent_engine_solve", C.c_int, [vp, C.c_double, C.c_int, C.c_int]),
     ("excent_engine_resume", C.c_int, [vp, C.c_double, C.c_int, C.c_int]),

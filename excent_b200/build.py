@@ -25,7 +25,10 @@ OBJ = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libexcent_b200.so")
 CLI = os.path.join(PKG, "bin", "excent")
 TOOLS = {"cli_main": CLI, "cli_params": os.path.join(PKG, "bin", "excent_params"),
-         "cli_reference": os.path.join(PKG, "bin", "excent_reference")}
+         "cli_reference": os.path.join(PKG, "bin", "excent_reference"),
+         "cli_convert": os.path.join(PKG, "bin", "excent_convert"),
+         "cli_info": os.path.join(PKG, "bin", "excent_info"),
+         "cli_evict": os.path.join(PKG, "bin", "excent_evict")}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 

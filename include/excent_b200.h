@@ -370,6 +370,30 @@ int excent_params_main(int argc, char** argv);
  * it (tools/centrality_reference.cu:71-214: same modes, files and lines). */
 int excent_reference_main(int argc, char** argv);
 
+/* ------------------------------------------------------------ EGR file tools */
+
+/* MatrixMarket coordinate file -> wide EGR (tools/efficient_converter.py:5-113).
+ * n = max(rows, cols) of the size line; every later line with at least two
+ * integer fields is an entry u v (1-based; further fields are ignored); entries
+ * whose source is past n are skipped, as the reference converter does; a
+ * source < 1 or a target outside [1, n] is EXCENT_ERR_IO. Lists keep the file's
+ * order unless flags ask otherwise: 1 sort each list, 2 sort and drop repeated
+ * entries, 4 drop self-loops, 8 add v -> u for every u -> v (u != v).
+ * stats (may be NULL): {n, entries read, skipped, self-loops read, m written}. */
+int excent_mtx_to_egr(const char* in, const char* out, int flags, unsigned long long* stats);
+/* One line on an EGR file: n, m, max degree, and 20000 entries sampled with
+ * mt19937_64 seeded 7 checked for a reverse entry and for self-loops; the same
+ * line tools/egr_info.cpp:10-30 prints. */
+int excent_egr_report(const char* path, char* out, int cap);
+/* bin/excent_convert in.mtx out.egr [--sort] [--dedup] [--no-self-loops] [--symmetric] */
+int excent_convert_main(int argc, char** argv);
+/* bin/excent_info graph.egr (the report line above). */
+int excent_info_main(int argc, char** argv);
+/* bin/excent_evict [--report] file...: drop files from the page cache
+ * (posix_fadvise DONTNEED after fdatasync) and print the resident share before
+ * and after, or only the share with --report (tools/evict_file.c:18-65). */
+int excent_evict_main(int argc, char** argv);
+
 /* ------------------------------------------------------------ batched solves */
 
 /* B personalized PageRank (kind EXCENT_PR: weight d / deg) or Katz (kind

@@ -62,6 +62,52 @@ def read_env(p):
     return env
 
 
+# A small MatrixMarket file with what real files hold: comments, a weight
+# column, repeated entries, self-loops, lists out of order, an empty vertex and
+# an entry whose source is past n (the reference converter skips it).
+EDGE_CASES_MTX = """%%MatrixMarket matrix coordinate real general
+% comment line
+7 6 14
+3 1 0.5
+1 2 1.0
+1 2 2.0
+2 2 1
+5 1
+9 3
+3 7
+2 1 4e-1
+1 6
+6 1
+1 1
+3 2
+7 3
+4 5
+"""
+
+
+def converter_goldens(meta):
+    """The reference's own converter (tools/efficient_converter.py, run here from the reference
+    checkout) on the sample's .mtx and on EDGE_CASES_MTX: golden EGR outputs."""
+    conv = os.path.join(os.path.dirname(os.path.dirname(REF)), "tools", "efficient_converter.py")
+    if not os.path.exists(conv):
+        return
+    edge = os.path.join(HERE, "edge_cases.mtx")
+    with open(edge, "w") as f:
+        f.write(EDGE_CASES_MTX)
+    # the sample's .mtx converts to exactly the sample's .egr: only its digest is kept
+    tmp = os.path.join(tempfile.mkdtemp(), "sample_converted.egr")
+    for src, dst in (("sample.mtx", tmp), ("edge_cases.mtx", os.path.join(HERE, "edge_cases_converted.egr"))):
+        subprocess.run([sys.executable, conv, os.path.join(HERE, src), dst], capture_output=True, text=True,
+                       check=True)
+        meta[f"efficient_converter {src}"] = sha(dst)
+    meta["edge_cases.mtx"] = sha(edge)
+    # the reference's egr_info line for the sample (oracle/_ref/egr_info, built from tools/egr_info.cpp)
+    info = os.path.join(REF_BIN, "egr_info")
+    if os.path.exists(info):
+        r = subprocess.run([info, os.path.join(HERE, "sample.egr")], capture_output=True, text=True, check=True)
+        meta["egr_info sample.egr"] = r.stdout.strip()
+
+
 def main():
     out_dir = HERE
     if "--out" in sys.argv:
@@ -70,10 +116,10 @@ def main():
     meta_p = os.path.join(out_dir, "golden.json")
     meta = json.load(open(meta_p)) if os.path.exists(meta_p) else {}
     if os.path.isdir(REF):
-        for f in ("sample.egr", "sample.env"):
+        for f in ("sample.egr", "sample.env", "sample.mtx"):
             shutil.copyfile(os.path.join(REF, f), os.path.join(HERE, f))
-        meta["sample.egr"] = sha(os.path.join(HERE, "sample.egr"))
-        meta["sample.env"] = sha(os.path.join(HERE, "sample.env"))
+            meta[f] = sha(os.path.join(HERE, f))
+        converter_goldens(meta)
     if "--gpu-ref" in sys.argv:
         egr = os.path.join(HERE, "sample.egr")
         env = read_env(os.path.join(HERE, "sample.env"))
