@@ -212,6 +212,10 @@ class Engine:
         code = {"table": 0, "first": 1, "last": 2, False: 0, True: 1}[order]
         call("excent_engine_set_hub_order", self.h, code)
 
+    def set_chunk_sweep(self, on=True):
+        """Cached pushes one chunk per launch, in chunk order (the reference's launch order)."""
+        call("excent_engine_set_chunk_sweep", self.h, int(bool(on)))
+
     def host_cache(self):
         """Pinned host memory for the entries past the edge cache (excent_engine_host_cache):
         returns (numpy int32 view to fill, first edge index)."""

@@ -67,6 +67,7 @@ PROTOS = [
     ("excent_engine_hot_pending", C.c_int, [vp, C.c_int, C.c_int, i32p, C.POINTER(C.c_uint)]),
     ("excent_engine_hot_edges", C.c_int, [vp, i32p]),
     ("excent_mtx_to_egr", C.c_int, [C.c_char_p, C.c_char_p, C.c_int, u64p]),
+    ("excent_engine_set_chunk_sweep", C.c_int, [vp, C.c_int]),
     ("excent_egr_report", C.c_int, [C.c_char_p, C.c_char_p, C.c_int]),
     ("excent_engine_sync", C.c_int, [vp]),
     ("excent_engine_solve", C.c_int, [vp, C.c_double, C.c_int, C.c_int]),
@@ -134,6 +135,9 @@ PROTOS = [
     ("excent_cli_main", C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
     ("excent_params_main", C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
     ("excent_reference_main", C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
+    ("excent_convert_main", C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
+    ("excent_info_main", C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
+    ("excent_evict_main", C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
     ("excent_rmat_generate", C.c_int, [C.c_int, C.c_int, C.c_int, u64, C.c_double, C.c_double, C.c_double,
                                        C.c_int, C.c_int, C.POINTER(vp)]),
     ("excent_ppr_fp64", C.c_int, [C.c_int, C.c_int, vp, vp, C.c_double, C.c_int, vp, vp, C.c_double, C.c_int, vp,

@@ -117,6 +117,7 @@ struct PushArgs {
     const int* hubv;
     const ull* hubv_cnt;
     int skip_hubs;      // SRC_TABLE leaves the lists longer than HUB_MIN to SRC_HUBS
+    int chunk;          // SRC_TABLE: only chunk `chunk`'s items (-1: every chunk's)
     // lists past the device cache read in place from pinned host memory (zero copy)
     const int* hcache;   // entries [cache_edges, m), device-mapped
     ull cache_edges;
@@ -402,11 +403,16 @@ __global__ void k_plan(int nc, const int* cv0, int n, ull* cnt, const uint8_t* c
 template <int SRC>
 __device__ __forceinline__ bool get_item(const PushArgs& a, long long t, int& v, const int*& nb, ull& deg) {
     if constexpr (SRC == SRC_TABLE) {
-        if (t >= (long long)a.wt_prefix[a.nc]) return false;
         int lo = 0, hi = a.nc - 1;  // chunk c with prefix[c] <= t < prefix[c+1]
-        while (lo < hi) {
-            int mid = (lo + hi + 1) >> 1;
-            if ((long long)a.wt_prefix[mid] <= t) lo = mid; else hi = mid - 1;
+        if (a.chunk >= 0) {
+            if (t >= (long long)a.wt_prefix[a.chunk + 1]) return false;
+            lo = a.chunk;
+        } else {
+            if (t >= (long long)a.wt_prefix[a.nc]) return false;
+            while (lo < hi) {
+                int mid = (lo + hi + 1) >> 1;
+                if ((long long)a.wt_prefix[mid] <= t) lo = mid; else hi = mid - 1;
+            }
         }
         const unsigned i = (unsigned)(t - a.wt_prefix[lo]);
         if (a.wt_type[lo] == WT_LIST) v = a.list[a.cv0[lo] + i];
@@ -454,9 +460,15 @@ __device__ __forceinline__ bool get_item(const PushArgs& a, long long t, int& v,
     }
 }
 
+// Items [item_first, item_total) of one launch.
+template <int SRC>
+__device__ __forceinline__ long long item_first(const PushArgs& a) {
+    if constexpr (SRC == SRC_TABLE) return a.chunk >= 0 ? a.wt_prefix[a.chunk] : 0;
+    else return 0;
+}
 template <int SRC>
 __device__ __forceinline__ long long item_total(const PushArgs& a) {
-    if constexpr (SRC == SRC_TABLE) return a.wt_prefix[a.nc];
+    if constexpr (SRC == SRC_TABLE) return a.wt_prefix[a.chunk >= 0 ? a.chunk + 1 : a.nc];
     else if constexpr (SRC == SRC_CHUNK) return a.ccount;
     else if constexpr (SRC == SRC_GATHER) return a.gk;
     else if constexpr (SRC == SRC_HUBS) return a.ctrl->pull ? 0 : (long long)*a.hubv_cnt;
@@ -484,15 +496,15 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    const long long total = item_total<SRC>(a);
+    const long long first = item_first<SRC>(a), total = item_total<SRC>(a);
     ull pushed = 0, hpushed = 0;
-    for (long long tile = gw; tile * 32 < total; tile += nwarps) {
+    for (long long tile = gw; first + tile * 32 < total; tile += nwarps) {
         int v = 0;
         const int* nb = nullptr;
         ull deg = 0;
         T p{};
         bool act = false;
-        if (get_item<SRC>(a, tile * 32 + lane, v, nb, deg) &&
+        if (get_item<SRC>(a, first + tile * 32 + lane, v, nb, deg) &&
             !(SRC == SRC_TABLE && a.skip_hubs && deg > HUB_MIN)) {   // pushed by SRC_HUBS
             p = take(x, r, v, deg, a.M);
             act = nonzero(p) && deg > 0;
@@ -836,6 +848,8 @@ __global__ void k_fill_hot(int lo, int hi, const int* hids, const ull* hoff, con
 }
 
 
+__global__ void k_reset_count(ull* c) { *c = 0; }
+
 // Vertices whose lists are longer than HUB_MIN, appended in any order.
 __global__ void k_hub_list(int n, const ull* idx, int* out, ull* cnt) {
     const int lane = threadIdx.x & 31;
@@ -952,6 +966,7 @@ struct excent_engine {
     ull* d_hubv_cnt = nullptr;
     ull hubv_cap = 0;
     int hub_order = 1;       // high-degree lists: 0 in table order, 1 first, 2 last
+    bool chunk_sweep = false; // cached pushes chunk by chunk, each launch after the previous one
     bool hubv_stale = true;
     double pull_frac = 0;    // pull when the pending demand >= pull_frac * m (0: never)
     bool ev_proj = false;
@@ -1355,7 +1370,7 @@ static PushArgs push_args(excent_engine* e, int q) {
     a.hids = e->d_hids; a.hoff = e->d_hoff; a.hedges = e->d_hedges; a.hlist = e->d_hlist;
     a.hubq = e->d_hubq[q]; a.hub_cap = e->hub_cap[q]; a.hub_cnt = e->d_hubcnt + q; a.ctrl = e->d_ctrl;
     a.hub_id = e->d_hub_id; a.hub_k = e->hub_k;
-    a.hubv = e->d_hubv; a.hubv_cnt = e->d_hubv_cnt; a.skip_hubs = 0;
+    a.hubv = e->d_hubv; a.hubv_cnt = e->d_hubv_cnt; a.skip_hubs = 0; a.chunk = -1;
     a.hcache = nullptr; a.cache_edges = e->cache_edges;
     if (e->h_hcache) cudaHostGetDevicePointer((void**)&a.hcache, e->h_hcache, 0);
     return a;
@@ -1406,7 +1421,17 @@ extern "C" int excent_engine_push_cached(excent_engine* e, const unsigned char* 
     EX_CUDA(cudaMemsetAsync(e->d_hubcnt, 0, sizeof(ull), e->s_main));
     PushArgs a = push_args(e, 0);
     a.hot = e->hot_skip ? e->d_hot : nullptr;
-    launch_push<SRC_TABLE>(e, a, grid_for(e, total), e->s_main);
+    if (e->chunk_sweep) {   // one launch (and its hub segments) per chunk, in chunk order
+        for (int c = 0; c < e->nc; c++) {
+            const unsigned items = e->h_wt_prefix[c + 1] - e->h_wt_prefix[c];
+            if (!items) continue;
+            a.chunk = c;
+            if (c) EX_CUDA(cudaMemsetAsync(e->d_hubcnt, 0, sizeof(ull), e->s_main));
+            launch_push<SRC_TABLE>(e, a, grid_for(e, items), e->s_main);
+        }
+    } else {
+        launch_push<SRC_TABLE>(e, a, grid_for(e, total), e->s_main);
+    }
     EX_CUDA(cudaGetLastError());
     return EXCENT_OK;
 }
@@ -1644,9 +1669,27 @@ static void enqueue_pass(excent_engine* e, double list_frac, int max_passes, cud
     };
     if (order == 1) hub_phase();
     a.skip_hubs = order != 0;   // the table push skips the high-degree vertices
-    if (e->L == 1) k_push<1, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
-    else k_push<4, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
-    e->launches++;
+    if (e->chunk_sweep) {
+        // chunk by chunk: each chunk's push (and, in table order, its hub segments) completes
+        // before the next chunk's vertices are taken, so they see everything pushed so far
+        for (int c = 0; c < e->nc; c++) {
+            a.chunk = c;
+            if (e->L == 1) k_push<1, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
+            else k_push<4, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
+            e->launches++;
+            if (order == 0 && c + 1 < e->nc) {
+                if (e->L == 1) k_hub<1><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
+                else k_hub<4><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
+                k_reset_count<<<1, 1, 0, st>>>(a.hub_cnt);
+                e->launches += 2;
+            }
+        }
+        a.chunk = -1;
+    } else {
+        if (e->L == 1) k_push<1, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
+        else k_push<4, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
+        e->launches++;
+    }
     if (pull_edges > 0) {   // each of these returns at once unless k_plan chose a pull pass
         if (e->L == 1) {
             k_take<1><<<gt, BLOCK, 0, st>>>(e->n, e->d_x, e->d_r, e->d_P, e->d_idx, e->M, e->d_ctrl);
@@ -2014,6 +2057,14 @@ extern "C" int excent_engine_set_hub_order(excent_engine* e, int order) {
     EX_CUDA(cudaSetDevice(e->dev));
     invalidate_graph(e);
     e->hub_order = order;
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_set_chunk_sweep(excent_engine* e, int on) {
+    EX_CHECK_ARG(e, "null engine");
+    EX_CUDA(cudaSetDevice(e->dev));
+    invalidate_graph(e);
+    e->chunk_sweep = on != 0;
     return EXCENT_OK;
 }
 

@@ -52,6 +52,7 @@ struct Options {
     int hub_targets = -1;      // shared-memory aggregation of the top-degree targets (-1: auto)
     int hub_order = 1;         // device loop: the high-degree lists 0 in table order, 1 first, 2 last
     std::string host_cache = "off";   // pinned: entries past the HBM cache read in place from pinned host memory
+    bool chunk_sweep = false;  // cached pushes one chunk per launch, in chunk order
 };
 
 static const char* USAGE =
@@ -120,6 +121,12 @@ static int parse_options(int argc, char** argv, Options& o) {
             if ((ok = next(v))) {
                 if (strcmp(v, "pinned") && strcmp(v, "off")) { fprintf(stderr, "--host-cache must be pinned or off\n"); return 1; }
                 o.host_cache = v;
+            }
+        }
+        else if (a == "--chunk-sweep") {
+            if ((ok = next(v))) {
+                if (strcmp(v, "on") && strcmp(v, "off")) { fprintf(stderr, "--chunk-sweep must be on or off\n"); return 1; }
+                o.chunk_sweep = !strcmp(v, "on");
             }
         }
         else if (a == "--hub-order") {
@@ -459,6 +466,7 @@ private:
             }
         }
         RT_CK(excent_engine_set_hub_order(e_, o_.hub_order));
+        RT_CK(excent_engine_set_chunk_sweep(e_, o_.chunk_sweep ? 1 : 0));
         hot_mode_ = cache_mode_ == "hot";
         if (hot_mode_) return setup_degree_cache(reserve);
         return 0;

@@ -242,6 +242,10 @@ int excent_engine_set_hub_targets(excent_engine* e, int k);
  * 0 in table order with the rest. No reference counterpart (the reference
  * pushes chunk by chunk, its degree cache at the end of a pass by default). */
 int excent_engine_set_hub_order(excent_engine* e, int order);
+/* Cached pushes chunk by chunk (on: one launch per chunk, each after the
+ * previous one, as the reference launches its resident chunks on one stream,
+ * src/excent.cu:684-688), or every chunk in one launch (off, the default). */
+int excent_engine_set_chunk_sweep(excent_engine* e, int on);
 
 /* Host cache for graphs larger than device memory: pinned, device-mapped host
  * memory for the entries past the HBM edge cache (entries [*first_edge, m),
