@@ -71,8 +71,6 @@ def parse():
     ap.add_argument("--ev-project", default="on", choices=["on", "off"],
                     help="FP64 eigenvector normalisation step (remove the principal-eigenvector component of the "
                          "eigenvector residual each pass); the `all` run does not reach eps 1e-6 at scale 24 without it")
-    ap.add_argument("--pull-frac", type=float, default=0.0,
-                    help="gather passes when the pending demand >= this fraction of the edges (0: always scatter)")
     ap.add_argument("--ref-gpu", action="store_true",
                     help="also run this repo's CLI and the reference CLI (built from source) on the same EGR file")
     ap.add_argument("--ref-passes", type=int, default=200, help="pass cap of the CLI runs for 'all'")
@@ -302,7 +300,6 @@ def run_ours(a, world, rank, local, dist):
     eng.upload_device(d_idx, d_adj)
     if v1 is not None and a.ev_project == "on":
         eng.ev_project(v1)
-    eng.set_pull(a.pull_frac)
     hub_k = a.hub_targets if a.hub_targets >= 0 else min(16384 if nm == 1 else 4096, n)
     eng.set_hub_targets(hub_k)
     eng.set_hub_order(a.hub_order)
@@ -394,7 +391,7 @@ def run_ours(a, world, rank, local, dist):
                    "l2_note": "inputs larger than L2 (edge cache %.2f GB)" % (m * 4 / 1e9),
                    "cuda_graph": use_graph, "parallelism": f"{world} independent replicas",
                    "ev_init": a.ev_init, "ev_project": a.ev_project if measure == "all" else None,
-                   "pull_frac": a.pull_frac, "hub_targets": hub_k, "list_frac": a.list_frac,
+                   "hub_targets": hub_k, "list_frac": a.list_frac,
                    "hub_order": a.hub_order},
         "e2e": {"value": round(e_pushed / te / 1e9, 4), "unit": "GTEPS", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": round(te / a.steps * 1e3, 3),

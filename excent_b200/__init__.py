@@ -233,10 +233,6 @@ class Engine:
         call("excent_engine_host_pushed", self.h, C.byref(v))
         return v.value
 
-    def set_pull(self, frac):
-        """Gather passes when the pending demand >= frac * m (symmetric graphs only; 0 = never)."""
-        call("excent_engine_set_pull", self.h, float(frac))
-
     def ev_project(self, v1):
         """FP64 eigenvector normalisation step with the unit principal eigenvector v1 (None: off)."""
         call("excent_engine_ev_project", self.h, _ptr(v1))

@@ -31,7 +31,7 @@ class Measures(C.Structure):
 
 class PassLog(C.Structure):
     _fields_ = [("pending", u64), ("demand", u64), ("hot_pending", u64), ("pushed", u64),
-                ("rsum", C.c_double * 3), ("n_list", C.c_int), ("n_range", C.c_int), ("pull", C.c_int)]
+                ("rsum", C.c_double * 3), ("n_list", C.c_int), ("n_range", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -108,7 +108,6 @@ PROTOS = [
     ("excent_wgraph_host_transposed", C.c_int, [vp]),
     ("excent_params_fp64", C.c_int, [C.c_int, C.c_int, vp, vp, C.c_double, f64p, vp]),
     ("excent_engine_ev_project", C.c_int, [vp, vp]),
-    ("excent_engine_set_pull", C.c_int, [vp, C.c_double]),
     ("excent_engine_set_hub_targets", C.c_int, [vp, C.c_int]),
     ("excent_engine_set_hub_order", C.c_int, [vp, C.c_int]),
     ("excent_engine_host_cache", C.c_int, [vp, C.POINTER(vp), u64p]),

@@ -44,20 +44,21 @@ struct Ctrl {
     int pass;          // passes that pushed so far
     int done;          // 1 once a snapshot found nothing pending (or max passes)
     int err;           // nonzero: a device-side capacity check failed
-    int pull;          // this pass gathers (pull) instead of scattering (push)
+    int pad0;
     double rsum[MAXM]; // FP64 sum |r| of the last snapshot
     unsigned hcount;   // hot pending list length
     unsigned pad2;
     double ev_dot;     // FP64 (r_ev . v1) accumulated by the snapshot
     double ev_corr;    // component removed from r_ev by the next snapshot
     ull host_pushed;   // entries pushed from lists read in place in host memory
+    ull chunk_runs;    // chunk launches a sweeping solve ran (chunks with items, summed over passes)
 };
 
 struct PassRec {
     ull pending, demand, hot_pending, pushed_before;
     double rsum[MAXM];
     int n_list, n_range;
-    int pull, pad;
+    int pad, pad1;
 };
 
 struct SnapArgs {
@@ -330,13 +331,13 @@ __global__ void __launch_bounds__(BLOCK) k_snapshot(SnapArgs a) {
 // next snapshot accumulates into, and set the graph's loop condition.
 __global__ void k_plan(int nc, const int* cv0, int n, ull* cnt, const uint8_t* cmode, double list_frac, int max_passes,
                        uint8_t* wt_type, unsigned* wt_prefix, Ctrl* ctrl, ull* hub_cnt, PassRec* log, int log_cap,
-                       cudaGraphConditionalHandle cond, int use_cond, double pull_edges) {
+                       cudaGraphConditionalHandle cond, int use_cond, const cudaGraphConditionalHandle* chunk_if) {
     __shared__ ull s_pend, s_dem;
     __shared__ unsigned s_carry;
-    __shared__ int s_nl, s_nr;
+    __shared__ int s_nl, s_nr, s_runs;
     __shared__ unsigned s_scan[1024];
     const int t = threadIdx.x;
-    if (t == 0) { s_pend = 0; s_dem = 0; s_carry = 0; s_nl = 0; s_nr = 0; }
+    if (t == 0) { s_pend = 0; s_dem = 0; s_carry = 0; s_nl = 0; s_nr = 0; s_runs = 0; }
     __syncthreads();
     ull lp = 0, ld = 0;
     for (int c = t; c < nc; c += blockDim.x) { lp += cnt[2 * c]; ld += cnt[2 * c + 1]; }
@@ -346,14 +347,12 @@ __global__ void k_plan(int nc, const int* cv0, int n, ull* cnt, const uint8_t* c
     const ull pend = s_pend, dem = s_dem, hp = ctrl->hotpend;
     const int p = ctrl->pass;
     const bool stop = ctrl->done || p >= max_passes || (pend == 0 && hp == 0);
-    // dense pass: gather over every list instead of scattering the pending ones
-    const bool pull = !stop && pull_edges > 0 && (double)dem >= pull_edges;
     // work table, scanned in tiles of blockDim.x chunks
     for (int base = 0; base < nc; base += blockDim.x) {
         const int c = base + t;
         unsigned items = 0;
         uint8_t ty = WT_NONE;
-        if (!stop && !pull && c < nc && cmode[c] && cnt[2 * c] > 0) {
+        if (!stop && c < nc && cmode[c] && cnt[2 * c] > 0) {
             const int v0 = cv0[c], v1 = c + 1 < nc ? cv0[c + 1] : n;
             // chunks read from host memory (mode 2) always push as ranges: a vertex that turns
             // pending during the pass is pushed in it, which saves whole passes over the link
@@ -370,7 +369,12 @@ __global__ void k_plan(int nc, const int* cv0, int n, ull* cnt, const uint8_t* c
             s_scan[t] += v;
             __syncthreads();
         }
-        if (c < nc) { wt_type[c] = ty; wt_prefix[c + 1] = s_carry + s_scan[t]; }
+        if (c < nc) {
+            wt_type[c] = ty;
+            wt_prefix[c + 1] = s_carry + s_scan[t];
+            if (chunk_if) cudaGraphSetConditional(chunk_if[c], items ? 1u : 0u);   // chunk sweep: launch it?
+            if (items) atomicAdd(&s_runs, 1);
+        }
         if (c == 0) wt_prefix[0] = 0;
         __syncthreads();
         if (t == blockDim.x - 1) s_carry += s_scan[t];
@@ -383,10 +387,9 @@ __global__ void k_plan(int nc, const int* cv0, int n, ull* cnt, const uint8_t* c
             R.pending = pend; R.demand = dem; R.hot_pending = hp; R.pushed_before = ctrl->pushed;
             for (int k = 0; k < MAXM; k++) R.rsum[k] = ctrl->rsum[k];
             R.n_list = s_nl; R.n_range = s_nr;
-            R.pull = pull;
         }
-        ctrl->pull = pull;
         ctrl->items = stop ? 0 : s_carry;
+        ctrl->chunk_runs += s_runs;
         if (stop) ctrl->done = 1; else ctrl->pass = p + 1;
         *hub_cnt = 0;
         ctrl->hotpend = 0;
@@ -471,7 +474,7 @@ __device__ __forceinline__ long long item_total(const PushArgs& a) {
     if constexpr (SRC == SRC_TABLE) return a.wt_prefix[a.chunk >= 0 ? a.chunk + 1 : a.nc];
     else if constexpr (SRC == SRC_CHUNK) return a.ccount;
     else if constexpr (SRC == SRC_GATHER) return a.gk;
-    else if constexpr (SRC == SRC_HUBS) return a.ctrl->pull ? 0 : (long long)*a.hubv_cnt;
+    else if constexpr (SRC == SRC_HUBS) return (long long)*a.hubv_cnt;
     else return a.ctrl->hcount;
 }
 
@@ -604,210 +607,9 @@ __global__ void __launch_bounds__(BLOCK) k_hub(void* rv, const HubSeg* q, const 
         const HubSeg h = q[s];
         T p;
         if constexpr (L == 1) p = h.p.x; else p = h.p;
-        if (!nonzero(p)) continue;   // a gather pass's segment (k_pullhub sums it)
         warp_scatter(r, h.nb, h.len, p, lane, hacc);
     }
     hacc_flush(hacc, r, hub_id, hub_k);
-}
-
-// ---------------------------------------------------------------- pull pass
-// A dense pass (pending demand >= a set fraction of the edges) runs as a
-// gather on symmetric graphs: k_take takes every pending vertex's residual
-// (plain loads and stores: nothing else touches r during the take) and writes
-// its per-entry weight P[v] (zero when not pending), then k_pull adds to each
-// vertex the weights of its neighbours, r[v] += sum_{u in N(v)} P[u], which is
-// what the scatter of every pending vertex would add. Lists longer than
-// HUB_MIN are summed in HUB_SEG-entry segments by k_pullhub.
-template <int L>
-__global__ void __launch_bounds__(BLOCK) k_take(int n, void* xv, void* rv, void* Pv, const ull* idx, DevMeasures M,
-                                                Ctrl* ctrl) {
-    typedef typename Lane<L>::T T;
-    if (!ctrl->pull) return;
-    T* x = reinterpret_cast<T*>(xv);
-    T* r = reinterpret_cast<T*>(rv);
-    T* P = reinterpret_cast<T*>(Pv);
-    __shared__ ull s_pushed[BLOCK / 32];
-    ull pushed = 0;
-    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
-        const ull deg = idx[v + 1] - idx[v];
-        T p;
-        if constexpr (L == 1) {
-            const float cur = r[v];
-            float d = 0.f;
-            if (fabsf(cur) > M.eps[0]) { d = cur; r[v] = 0.f; x[v] += d; }
-            p = deg ? weight(d, deg, M, 0) : 0.f;
-            if (d != 0.f && deg) pushed += deg;
-        } else {
-            float4 cur = r[v];
-            float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (fabsf(cur.x) > M.eps[0]) { d.x = cur.x; cur.x = 0.f; }
-            if (M.nm > 1 && fabsf(cur.y) > M.eps[1]) { d.y = cur.y; cur.y = 0.f; }
-            if (M.nm > 2 && fabsf(cur.z) > M.eps[2]) { d.z = cur.z; cur.z = 0.f; }
-            if (nonzero(d)) {
-                r[v] = cur;
-                float4 xv4 = x[v];
-                xv4.x += d.x; xv4.y += d.y; xv4.z += d.z;
-                x[v] = xv4;
-                if (deg) pushed += deg;
-            }
-            p = deg ? make_float4(weight(d.x, deg, M, 0), weight(d.y, deg, M, 1), weight(d.z, deg, M, 2), 0.f)
-                    : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        P[v] = p;
-    }
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    pushed = warp_sum(pushed);
-    if (lane == 0) s_pushed[wib] = pushed;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        ull t = 0;
-        for (int i = 0; i < BLOCK / 32; i++) t += s_pushed[i];
-        if (t) atomicAdd(&ctrl->pushed, t);
-    }
-}
-
-__device__ __forceinline__ float shfl_up(float v, int d) { return __shfl_up_sync(FULL, v, d); }
-__device__ __forceinline__ float4 shfl_up(float4 v, int d) {
-    return make_float4(__shfl_up_sync(FULL, v.x, d), __shfl_up_sync(FULL, v.y, d), __shfl_up_sync(FULL, v.z, d),
-                       __shfl_up_sync(FULL, v.w, d));
-}
-__device__ __forceinline__ void acc_add(float& a, float b) { a += b; }
-__device__ __forceinline__ void acc_add(float4& a, float4 b) { a.x += b.x; a.y += b.y; a.z += b.z; a.w += b.w; }
-template <typename T> __device__ __forceinline__ T zero_of();
-template <> __device__ __forceinline__ float zero_of<float>() { return 0.f; }
-template <> __device__ __forceinline__ float4 zero_of<float4>() { return make_float4(0.f, 0.f, 0.f, 0.f); }
-
-// A gather pass walks a static table built once per graph: tiles of whole
-// 32-vertex groups holding about PULL_TILE entries each (lists longer than
-// HUB_MIN excluded), and segments of HUB_SEG entries of those long lists.
-// Every warp gets the same amount of work, with no queue or atomics.
-static constexpr unsigned PULL_TILE = 4096;
-struct PullTile { unsigned g0, ng; };           // groups [g0, g0 + ng) of 32 vertices
-struct PullSeg { ull b; unsigned len; int v; };  // entries [b, b + len) of v's list
-
-template <int L>
-__global__ void __launch_bounds__(BLOCK) k_pull(int n, void* rv, const void* Pv, const ull* idx, const int* cache,
-                                                const PullTile* tiles, int ntiles, Ctrl* ctrl, const int* hub_id) {
-    typedef typename Lane<L>::T T;
-    if (!ctrl->pull) return;
-    T* r = reinterpret_cast<T*>(rv);
-    const T* P = reinterpret_cast<const T*>(Pv);
-    __shared__ const int* s_nb[BLOCK / 32][32];
-    __shared__ unsigned s_ex[BLOCK / 32][32];
-    __shared__ T s_acc[BLOCK / 32][32];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    const unsigned le = lane == 31 ? FULL : (2u << lane) - 1u;   // lanes <= this one
-    for (long long t = gw; t < ntiles; t += nwarps) {
-        const PullTile tl = tiles[t];
-        for (unsigned g = tl.g0; g < tl.g0 + tl.ng; g++) {
-            const long long v = (long long)g * 32 + lane;
-            ull b = 0, deg = 0;
-            if (v < n) { b = idx[v]; deg = idx[v + 1] - b; }
-            const unsigned ds = deg > HUB_MIN ? 0u : (unsigned)deg;   // long lists: segments
-            const unsigned nz = __ballot_sync(FULL, ds != 0);
-            if (!nz) continue;
-            // the group's nonempty lists in lane order, indexed by their rank among them
-            const int rank = __popc(nz & ((1u << lane) - 1u));
-            const unsigned incl = warp_incl_scan(ds, lane);
-            const unsigned tot = __shfl_sync(FULL, incl, 31);
-            const unsigned ex = incl - ds;
-            if (ds) { s_nb[wib][rank] = cache + b; s_ex[wib][rank] = ex; s_acc[wib][rank] = zero_of<T>(); }
-            __syncwarp();
-            for (unsigned j0 = 0; j0 < tot; j0 += 32 * UNROLL) {
-                T val[UNROLL];
-                int own[UNROLL], dist[UNROLL];
-                bool last[UNROLL];
-#pragma unroll
-                for (int k = 0; k < UNROLL; k++) {
-                    // window [wb, wb+32) of the concatenated lists: bit i of `starts` marks a list
-                    // beginning at entry wb+i; the owner of entry wb is the last list starting at or
-                    // before it, so lane i's owner is that one plus the starts in (wb, wb+i].
-                    const unsigned wb = j0 + 32 * k;
-                    const unsigned j = wb + lane;
-                    const unsigned starts =
-                        __reduce_or_sync(FULL, (ds && ex >= wb && ex - wb < 32) ? 1u << (ex - wb) : 0u);
-                    const int o0 = __popc(__ballot_sync(FULL, ds && ex <= wb)) - 1;
-                    const unsigned sl = starts & le;
-                    own[k] = o0 + __popc(sl & ~1u);
-                    dist[k] = sl ? lane - (31 - __clz(sl)) : lane;
-                    last[k] = j < tot && (lane == 31 || j + 1 == tot || ((starts >> (lane + 1)) & 1u));
-                    val[k] = zero_of<T>();
-                    if (j < tot) {
-                        int u = ld_edge(s_nb[wib][own[k]] + (j - s_ex[wib][own[k]]));
-                        if (u < 0) u = hub_id[u & HUB_MASK];
-                        val[k] = __ldg(P + u);
-                    }
-                }
-#pragma unroll
-                for (int k = 0; k < UNROLL; k++) {
-                    // segmented inclusive sum: lane i adds the lanes of its own list below it
-                    T sv = val[k];
-#pragma unroll
-                    for (int d = 1; d < 32; d <<= 1) {
-                        const T tv = shfl_up(sv, d);
-                        if (d <= dist[k]) acc_add(sv, tv);
-                    }
-                    if (last[k]) acc_add(s_acc[wib][own[k]], sv);
-                    __syncwarp();
-                }
-            }
-            if (ds) {
-                const T add = s_acc[wib][rank];
-                if (nonzero(add)) {   // this warp owns v: plain read-modify-write
-                    T cur = r[v];
-                    acc_add(cur, add);
-                    r[v] = cur;
-                }
-            }
-            __syncwarp();
-        }
-    }
-}
-
-// The long lists' segments: one warp sums the weights of a segment's entries
-// and adds the sum to the segment's vertex (segments of one list may run on
-// several warps, hence the reduction).
-template <int L>
-__global__ void __launch_bounds__(BLOCK) k_pullhub(void* rv, const void* Pv, const int* cache, const PullSeg* segs,
-                                                   int nseg, const Ctrl* ctrl, const int* hub_id) {
-    typedef typename Lane<L>::T T;
-    if (!ctrl->pull) return;
-    T* r = reinterpret_cast<T*>(rv);
-    const T* P = reinterpret_cast<const T*>(Pv);
-    const int lane = threadIdx.x & 31;
-    const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long s = gw; s < nseg; s += nwarps) {
-        const PullSeg h = segs[s];
-        const int* nb = cache + h.b;
-        T acc = zero_of<T>();
-        const unsigned mis = (unsigned)(((uintptr_t)nb >> 2) & 3u);
-        unsigned head = (4u - mis) & 3u;
-        if (head > h.len) head = h.len;
-        auto dec = [&](int u) { return u < 0 ? hub_id[u & HUB_MASK] : u; };
-        if (lane < (int)head) acc_add(acc, __ldg(P + dec(ld_edge(nb + lane))));
-        const int4* body = reinterpret_cast<const int4*>(nb + head);
-        const unsigned nbody = (h.len - head) >> 2;
-        unsigned i = lane;
-        for (; i + 32 < nbody; i += 64) {   // two 128-bit index loads in flight per lane
-            const int4 e0 = ld_edge4(body + i), e1 = ld_edge4(body + i + 32);
-            const T a0 = __ldg(P + dec(e0.x)), a1 = __ldg(P + dec(e0.y)), a2 = __ldg(P + dec(e0.z)), a3 = __ldg(P + dec(e0.w));
-            const T b0 = __ldg(P + dec(e1.x)), b1 = __ldg(P + dec(e1.y)), b2 = __ldg(P + dec(e1.z)), b3 = __ldg(P + dec(e1.w));
-            acc_add(acc, a0); acc_add(acc, a1); acc_add(acc, a2); acc_add(acc, a3);
-            acc_add(acc, b0); acc_add(acc, b1); acc_add(acc, b2); acc_add(acc, b3);
-        }
-        for (; i < nbody; i += 32) {
-            const int4 e = ld_edge4(body + i);
-            const T a0 = __ldg(P + dec(e.x)), a1 = __ldg(P + dec(e.y)), a2 = __ldg(P + dec(e.z)), a3 = __ldg(P + dec(e.w));
-            acc_add(acc, a0); acc_add(acc, a1); acc_add(acc, a2); acc_add(acc, a3);
-        }
-        const unsigned tail = (h.len - head) & 3u;
-        if (lane < (int)tail) acc_add(acc, __ldg(P + dec(ld_edge(nb + head + nbody * 4 + lane))));
-        acc = warp_sum(acc);
-        if (lane == 0 && nonzero(acc)) red_add(r, h.v, acc);
-    }
 }
 
 // Pending hot vertices among hot ids [lo, hi) at launch time, appended with
@@ -847,8 +649,6 @@ __global__ void k_fill_hot(int lo, int hi, const int* hids, const ull* hoff, con
     for (ull i = lane, d = hoff[w + 1] - hoff[w]; i < d; i += 32) to[i] = from[i];
 }
 
-
-__global__ void k_reset_count(ull* c) { *c = 0; }
 
 // Vertices whose lists are longer than HUB_MIN, appended in any order.
 __global__ void k_hub_list(int n, const ull* idx, int* out, ull* cnt) {
@@ -953,11 +753,6 @@ struct excent_engine {
     bool trace_on = false;
     float* d_tmp = nullptr;  // n floats for readback of the float4 layout
     float* d_v1 = nullptr;   // unit principal eigenvector for the EV normalisation step
-    void* d_P = nullptr;     // per-vertex push weights of a pull pass
-    PullTile* d_ptiles = nullptr;   // static work table of gather passes
-    PullSeg* d_psegs = nullptr;
-    int n_ptiles = 0, n_psegs = 0;
-    bool pull_stale = true;
     int* d_hub_id = nullptr; // hub-target aggregation: vertex of each slot
     int hub_k = 0;           // slots in use (0: off)
     int* h_hcache = nullptr; // pinned, mapped host copy of the entries past the device cache
@@ -967,8 +762,9 @@ struct excent_engine {
     ull hubv_cap = 0;
     int hub_order = 1;       // high-degree lists: 0 in table order, 1 first, 2 last
     bool chunk_sweep = false; // cached pushes chunk by chunk, each launch after the previous one
+    cudaGraphConditionalHandle* d_chunk_if = nullptr;  // per chunk: does this pass push it (graph IF nodes)
+    std::vector<cudaGraphConditionalHandle> h_chunk_if;
     bool hubv_stale = true;
-    double pull_frac = 0;    // pull when the pending demand >= pull_frac * m (0: never)
     bool ev_proj = false;
     int ev_index = -1;
     int* d_cache = nullptr;
@@ -1017,7 +813,7 @@ static int free_engine(excent_engine* e) {
     cudaDeviceSynchronize();
     if (e->gexec) cudaGraphExecDestroy(e->gexec);
     if (e->graph) cudaGraphDestroy(e->graph);
-    void* dptrs[] = {e->d_ptiles, e->d_psegs, e->d_hub_id, e->d_hubv, e->d_hubv_cnt, e->d_P, e->d_v1, e->d_idx, e->d_x, e->d_r, e->d_bitmap, e->d_cnt, e->d_cv0, e->d_list, e->d_ctrl, e->d_cmode,
+    void* dptrs[] = {e->d_chunk_if, e->d_hub_id, e->d_hubv, e->d_hubv_cnt, e->d_v1, e->d_idx, e->d_x, e->d_r, e->d_bitmap, e->d_cnt, e->d_cv0, e->d_list, e->d_ctrl, e->d_cmode,
                      e->d_wt_type, e->d_wt_prefix, e->d_hubq[0], e->d_hubq[1], e->d_hubq[2], e->d_hubcnt, e->d_log, e->d_trace, e->d_tmp, e->d_cache,
                      e->d_hids, e->d_hoff, e->d_hedges, e->d_hot, e->d_hlist};
     for (void* p : dptrs) if (p) cudaFree(p);
@@ -1186,7 +982,6 @@ extern "C" int excent_engine_upload_offsets(excent_engine* e, const unsigned lon
     EX_CUDA(cudaMemcpyAsync(e->d_idx + v0, idx, count * sizeof(ull), cudaMemcpyHostToDevice, e->s_main));
     EX_CUDA(cudaStreamSynchronize(e->s_main));
     e->hubv_stale = true;
-    e->pull_stale = true;
     return EXCENT_OK;
 }
 
@@ -1200,7 +995,6 @@ extern "C" int excent_engine_upload_device(excent_engine* e, const unsigned long
     EX_CUDA(cudaStreamSynchronize(e->s_main));
     EX_CUDA(cudaGetLastError());
     e->hubv_stale = true;
-    e->pull_stale = true;
     std::fill(e->loaded.begin(), e->loaded.end(), 1);
     return EXCENT_OK;
 }
@@ -1637,25 +1431,79 @@ extern "C" int excent_engine_sync(excent_engine* e) {
     return EXCENT_OK;
 }
 
-// One pass of the device solve: snapshot -> plan -> push -> hubs. With ev,
-// events are recorded between the kernels.
-static void enqueue_pass(excent_engine* e, double list_frac, int max_passes, cudaGraphConditionalHandle cond,
-                         int use_cond, cudaStream_t st, cudaEvent_t* ev = nullptr) {
+// Open an IF node on the stream being captured (condition `h`, set per pass
+// by k_plan) and start capturing its body on `body`; close_if ends the body.
+static cudaError_t open_if(cudaStream_t st, cudaStream_t body, cudaGraphConditionalHandle* h) {
+    cudaStreamCaptureStatus status;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    cudaError_t rc = cudaStreamGetCaptureInfo(st, &status, nullptr, &g, &deps, &nd);
+    if (rc != cudaSuccess) return rc;
+    if (status != cudaStreamCaptureStatusActive) return cudaErrorStreamCaptureInvalidated;
+    rc = cudaGraphConditionalHandleCreate(h, g, 0, cudaGraphCondAssignDefault);
+    if (rc != cudaSuccess) return rc;
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = *h;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    rc = cudaGraphAddNode(&node, g, deps, nd, &cp);
+    if (rc != cudaSuccess) return rc;
+    rc = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
+    if (rc != cudaSuccess) return rc;
+    return cudaStreamBeginCaptureToGraph(body, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeRelaxed);
+}
+static cudaError_t close_if(cudaStream_t body) {
+    cudaGraph_t g = nullptr;
+    return cudaStreamEndCapture(body, &g);
+}
+
+// Kernels of one pass outside the per-chunk launches of a chunk sweep, and per
+// chunk launch (for the launch count of a graph solve).
+static void pass_kernels(const excent_engine* e, int order, ull* fixed, ull* per_chunk) {
+    *fixed = 2 + (order == 1 || order == 2 ? 2 : 0) + (e->chunk_sweep ? 0 : (order == 0 ? 2 : 1));
+    *per_chunk = e->chunk_sweep ? (order == 0 ? 2 : 1) : 0;
+}
+
+static int effective_order(const excent_engine* e) {
+    return e->hub_order && e->d_hubv && !e->hubv_stale ? e->hub_order : 0;
+}
+
+// One pass of the device solve: snapshot -> plan -> push -> hub segments.
+// With ev, events are recorded between the kernels. chunk_body (a second
+// stream) is given while the pass is captured into a graph with a chunk
+// sweep: each chunk's launches then sit in an IF node that k_plan switches
+// off for chunks with nothing to push; e->h_chunk_if receives the handles.
+static cudaError_t enqueue_pass(excent_engine* e, double list_frac, int max_passes, cudaGraphConditionalHandle cond,
+                                int use_cond, cudaStream_t st, cudaEvent_t* ev = nullptr,
+                                cudaStream_t chunk_body = nullptr) {
     if (ev) cudaEventRecord(ev[0], st);
     launch_snapshot(e, false, st);
     if (ev) cudaEventRecord(ev[1], st);
-    const double pull_edges = e->pull_frac > 0 && e->d_P && !e->h_hcache ? e->pull_frac * (double)e->m : 0.0;
+    const bool use_if = chunk_body && e->chunk_sweep;
     k_plan<<<1, 1024, 0, st>>>(e->nc, e->d_cv0, e->n, e->d_cnt, e->d_cmode, list_frac, max_passes, e->d_wt_type,
                                e->d_wt_prefix, e->d_ctrl, e->d_hubcnt, e->d_log, e->log_cap, cond, use_cond,
-                               pull_edges);
+                               use_if ? e->d_chunk_if : nullptr);
     e->launches++;
     if (ev) cudaEventRecord(ev[2], st);
     PushArgs a = push_args(e, 0);
-    const int gt = e->sms * 8;
     // high-degree order: 1 = the lists longer than HUB_MIN first, so their (large) share of the
     // pass's residual reaches every other vertex before that vertex is taken; 2 = last, so they
     // collect the pass's residual and push it once; 0 = in table order with the rest
-    const int order = e->hub_order && e->d_hubv && !e->hubv_stale ? e->hub_order : 0;
+    const int order = effective_order(e);
+    auto hubs = [&](cudaStream_t s) {
+        if (e->L == 1) k_hub<1><<<e->grid_push, BLOCK, hub_smem(e), s>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
+        else k_hub<4><<<e->grid_push, BLOCK, hub_smem(e), s>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
+        e->launches++;
+    };
+    auto table = [&](cudaStream_t s) {
+        if (e->L == 1) k_push<1, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), s>>>(a);
+        else k_push<4, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), s>>>(a);
+        e->launches++;
+    };
     auto hub_phase = [&]() {
         // every list of SRC_HUBS is longer than HUB_MIN, so this push only takes and queues:
         // no entry is scattered here and the hub-target slots are not needed
@@ -1663,9 +1511,8 @@ static void enqueue_pass(excent_engine* e, double list_frac, int max_passes, cud
         ah.hub_k = 0;
         if (e->L == 1) k_push<1, SRC_HUBS><<<e->grid_push, BLOCK, 0, st>>>(ah);
         else k_push<4, SRC_HUBS><<<e->grid_push, BLOCK, 0, st>>>(ah);
-        if (e->L == 1) k_hub<1><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
-        else k_hub<4><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
-        e->launches += 2;
+        e->launches++;
+        hubs(st);
     };
     if (order == 1) hub_phase();
     a.skip_hubs = order != 0;   // the table push skips the high-degree vertices
@@ -1674,56 +1521,38 @@ static void enqueue_pass(excent_engine* e, double list_frac, int max_passes, cud
         // before the next chunk's vertices are taken, so they see everything pushed so far
         for (int c = 0; c < e->nc; c++) {
             a.chunk = c;
-            if (e->L == 1) k_push<1, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
-            else k_push<4, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
-            e->launches++;
-            if (order == 0 && c + 1 < e->nc) {
-                if (e->L == 1) k_hub<1><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
-                else k_hub<4><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
-                k_reset_count<<<1, 1, 0, st>>>(a.hub_cnt);
-                e->launches += 2;
+            cudaStream_t s = st;
+            if (use_if) {
+                const cudaError_t rc = open_if(st, chunk_body, &e->h_chunk_if[c]);
+                if (rc != cudaSuccess) return rc;
+                s = chunk_body;
+            }
+            table(s);
+            if (order == 0) {
+                hubs(s);
+                cudaMemsetAsync(a.hub_cnt, 0, sizeof(ull), s);
+            }
+            if (use_if) {
+                const cudaError_t rc = close_if(chunk_body);
+                if (rc != cudaSuccess) return rc;
             }
         }
         a.chunk = -1;
     } else {
-        if (e->L == 1) k_push<1, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
-        else k_push<4, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
-        e->launches++;
-    }
-    if (pull_edges > 0) {   // each of these returns at once unless k_plan chose a pull pass
-        if (e->L == 1) {
-            k_take<1><<<gt, BLOCK, 0, st>>>(e->n, e->d_x, e->d_r, e->d_P, e->d_idx, e->M, e->d_ctrl);
-            k_pull<1><<<e->grid_push, BLOCK, 0, st>>>(e->n, e->d_r, e->d_P, e->d_idx, e->d_cache, e->d_ptiles,
-                                                       e->n_ptiles, e->d_ctrl, e->d_hub_id);
-        } else {
-            k_take<4><<<gt, BLOCK, 0, st>>>(e->n, e->d_x, e->d_r, e->d_P, e->d_idx, e->M, e->d_ctrl);
-            k_pull<4><<<e->grid_push, BLOCK, 0, st>>>(e->n, e->d_r, e->d_P, e->d_idx, e->d_cache, e->d_ptiles,
-                                                       e->n_ptiles, e->d_ctrl, e->d_hub_id);
-        }
-        e->launches += 2;
+        table(st);
     }
     if (ev) cudaEventRecord(ev[3], st);
-    if (order == 0) {   // the table push's own segments (with a high-degree order it queues none)
-        if (e->L == 1) k_hub<1><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
-        else k_hub<4><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
-        e->launches++;
-    }
+    if (order == 0 && !e->chunk_sweep) hubs(st);   // the table push's own segments
     if (order == 2) hub_phase();
-    if (pull_edges > 0) {
-        if (e->L == 1)
-            k_pullhub<1><<<e->grid_push, BLOCK, 0, st>>>(e->d_r, e->d_P, e->d_cache, e->d_psegs, e->n_psegs, e->d_ctrl,
-                                                          e->d_hub_id);
-        else
-            k_pullhub<4><<<e->grid_push, BLOCK, 0, st>>>(e->d_r, e->d_P, e->d_cache, e->d_psegs, e->n_psegs, e->d_ctrl,
-                                                          e->d_hub_id);
-        e->launches++;
-    }
     if (ev) cudaEventRecord(ev[4], st);
+    return cudaGetLastError();
 }
 
 static int build_graph(excent_engine* e, double list_frac, int max_passes) {
     if (e->gexec && e->graph_max_passes == max_passes && e->graph_list_frac == list_frac) return EXCENT_OK;
     invalidate_graph(e);
+    if (e->chunk_sweep && !e->d_chunk_if) EX_ALLOC(e->d_chunk_if, (size_t)e->nc * sizeof(cudaGraphConditionalHandle));
+    e->h_chunk_if.assign(e->nc, 0);
     cudaGraph_t g;
     EX_CUDA(cudaGraphCreate(&g, 0));
     cudaGraphConditionalHandle h;
@@ -1737,17 +1566,27 @@ static int build_graph(excent_engine* e, double list_frac, int max_passes) {
     EX_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     // capture one pass into the body graph
-    cudaStream_t cs;
+    cudaStream_t cs, cb;
     EX_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    EX_CUDA(cudaStreamCreateWithFlags(&cb, cudaStreamNonBlocking));
     EX_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     const ull before = e->launches;
-    enqueue_pass(e, list_frac, max_passes, h, 1, cs);
+    const cudaError_t pe = enqueue_pass(e, list_frac, max_passes, h, 1, cs, nullptr, e->chunk_sweep ? cb : nullptr);
     e->launches = before;
     cudaGraph_t captured;
-    cudaError_t ce = cudaStreamEndCapture(cs, &captured);
+    const cudaError_t ce = cudaStreamEndCapture(cs, &captured);
     cudaStreamDestroy(cs);
-    EX_CUDA(ce);
-    EX_CUDA(cudaGraphInstantiate(&e->gexec, g, 0));
+    cudaStreamDestroy(cb);
+    if (pe != cudaSuccess || ce != cudaSuccess) {
+        cudaGraphDestroy(g);
+        cudaGetLastError();
+        EX_CUDA(pe != cudaSuccess ? pe : ce);
+    }
+    if (e->chunk_sweep)
+        EX_CUDA(cudaMemcpy(e->d_chunk_if, e->h_chunk_if.data(), (size_t)e->nc * sizeof(cudaGraphConditionalHandle),
+                           cudaMemcpyHostToDevice));
+    const cudaError_t ie = cudaGraphInstantiate(&e->gexec, g, 0);
+    if (ie != cudaSuccess) { cudaGraphDestroy(g); e->gexec = nullptr; EX_CUDA(ie); }
     e->graph = g;
     e->graph_max_passes = max_passes;
     e->graph_list_frac = list_frac;
@@ -1790,48 +1629,6 @@ extern "C" int excent_engine_seed(excent_engine* e, int k, const int32_t* vids, 
     return EXCENT_OK;
 }
 
-// The static work table of gather passes (from the offsets, once per graph).
-static int build_pull_tables(excent_engine* e) {
-    std::vector<ull> idx((size_t)e->n + 1);
-    EX_CUDA(cudaMemcpy(idx.data(), e->d_idx, idx.size() * sizeof(ull), cudaMemcpyDeviceToHost));
-    std::vector<PullTile> tiles;
-    std::vector<PullSeg> segs;
-    const unsigned ng = (unsigned)(((ull)e->n + 31) / 32);
-    ull acc = 0;
-    unsigned g0 = 0;
-    for (unsigned g = 0; g < ng; g++) {
-        const ull v0 = (ull)g * 32, v1 = std::min<ull>(v0 + 32, (ull)e->n);
-        for (ull v = v0; v < v1; v++) {
-            const ull d = idx[v + 1] - idx[v];
-            if (d > HUB_MIN) {
-                for (ull o = 0; o < d; o += HUB_SEG)
-                    segs.push_back(PullSeg{idx[v] + o, (unsigned)std::min<ull>(HUB_SEG, d - o), (int)v});
-            } else {
-                acc += d;
-            }
-        }
-        acc += 32;   // the group's offsets and bookkeeping
-        if (acc >= PULL_TILE || g + 1 == ng) {
-            tiles.push_back(PullTile{g0, g + 1 - g0});
-            g0 = g + 1;
-            acc = 0;
-        }
-    }
-    invalidate_graph(e);
-    if (e->d_ptiles) cudaFree(e->d_ptiles);
-    if (e->d_psegs) cudaFree(e->d_psegs);
-    e->d_ptiles = nullptr;
-    e->d_psegs = nullptr;
-    EX_ALLOC(e->d_ptiles, std::max<size_t>(tiles.size(), 1) * sizeof(PullTile));
-    EX_ALLOC(e->d_psegs, std::max<size_t>(segs.size(), 1) * sizeof(PullSeg));
-    if (!tiles.empty()) EX_CUDA(cudaMemcpy(e->d_ptiles, tiles.data(), tiles.size() * sizeof(PullTile), cudaMemcpyHostToDevice));
-    if (!segs.empty()) EX_CUDA(cudaMemcpy(e->d_psegs, segs.data(), segs.size() * sizeof(PullSeg), cudaMemcpyHostToDevice));
-    e->n_ptiles = (int)tiles.size();
-    e->n_psegs = (int)segs.size();
-    e->pull_stale = false;
-    return EXCENT_OK;
-}
-
 static int solve_impl(excent_engine* e, double list_frac, int max_passes, int use_graph, bool init) {
     EX_CHECK_ARG(e, "null engine");
     EX_CHECK_ARG(max_passes >= 0 && max_passes < e->log_cap, "max_passes must be < %d", e->log_cap);
@@ -1845,7 +1642,6 @@ static int solve_impl(excent_engine* e, double list_frac, int max_passes, int us
     EX_CUDA(cudaMemcpy(e->d_cmode, cm.data(), e->nc, cudaMemcpyHostToDevice));
     if (init) EX_TRY(init_state(e));
     else EX_TRY(reset_counters(e));
-    if (e->pull_frac > 0 && e->d_P && !e->h_hcache && e->pull_stale) EX_TRY(build_pull_tables(e));
     if (e->hub_order && e->hubv_stale) {
         // count the high-degree vertices, then list them in a buffer of that size
         if (!e->d_hubv_cnt) EX_ALLOC(e->d_hubv_cnt, sizeof(ull));
@@ -1879,12 +1675,12 @@ static int solve_impl(excent_engine* e, double list_frac, int max_passes, int us
         EX_CUDA(cudaGraphLaunch(e->gexec, e->s_main));
         EX_CUDA(cudaStreamSynchronize(e->s_main));
         EX_CUDA(cudaMemcpy(e->h_ctrl, e->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
-        e->launches += ((e->pull_frac > 0 && e->d_P ? 7ull : 4ull) + (e->hub_order && e->d_hubv ? 1ull : 0ull)) *
-                       (e->h_ctrl->pass + 1);
+        ull fixed = 0, per_chunk = 0;
+        pass_kernels(e, effective_order(e), &fixed, &per_chunk);
+        e->launches += fixed * (e->h_ctrl->pass + 1) + per_chunk * e->h_ctrl->chunk_runs;
     } else {
         for (int p = 0; p <= max_passes; p++) {
-            enqueue_pass(e, list_frac, max_passes, 0, 0, e->s_main, e->prof ? e->ev : nullptr);
-            EX_CUDA(cudaGetLastError());
+            EX_CUDA(enqueue_pass(e, list_frac, max_passes, 0, 0, e->s_main, e->prof ? e->ev : nullptr));
             EX_CUDA(cudaMemcpyAsync(e->h_ctrl, e->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, e->s_main));
             EX_CUDA(cudaStreamSynchronize(e->s_main));
             if (e->prof && !e->h_ctrl->done) {
@@ -1929,7 +1725,6 @@ extern "C" int excent_engine_stats(excent_engine* e, excent_stats* st, excent_pa
             L.pushed = (p + 1 < np ? recs[p + 1].pushed_before : c.pushed) - recs[p].pushed_before;
             for (int k = 0; k < MAXM; k++) L.rsum[k] = recs[p].rsum[k];
             L.n_list = recs[p].n_list; L.n_range = recs[p].n_range;
-            L.pull = recs[p].pull;
         }
     }
     return EXCENT_OK;
@@ -2093,15 +1888,6 @@ extern "C" int excent_engine_host_pushed(excent_engine* e, unsigned long long* e
     EX_CUDA(cudaSetDevice(e->dev));
     EX_CUDA(cudaStreamSynchronize(e->s_main));
     EX_CUDA(cudaMemcpy(entries, &e->d_ctrl->host_pushed, sizeof(ull), cudaMemcpyDeviceToHost));
-    return EXCENT_OK;
-}
-
-extern "C" int excent_engine_set_pull(excent_engine* e, double pull_frac) {
-    EX_CHECK_ARG(e && pull_frac >= 0, "bad argument");
-    EX_CUDA(cudaSetDevice(e->dev));
-    invalidate_graph(e);
-    if (pull_frac > 0 && !e->d_P) EX_ALLOC(e->d_P, (size_t)e->n * (e->L == 1 ? sizeof(float) : sizeof(float4)));
-    e->pull_frac = pull_frac;
     return EXCENT_OK;
 }
 

@@ -197,7 +197,6 @@ typedef struct excent_pass_log {
     unsigned long long pushed;    /* adjacency entries pushed in the pass */
     double rsum[3];               /* FP64 sum of |r| per measure at the snapshot */
     int n_list, n_range;          /* chunks pushed as lists / whole ranges */
-    int pull;                     /* 1: the pass ran as a gather (excent_engine_set_pull) */
 } excent_pass_log;
 
 typedef struct excent_stats {
@@ -257,17 +256,6 @@ int excent_engine_set_chunk_sweep(excent_engine* e, int on);
 int excent_engine_host_cache(excent_engine* e, int32_t** host_edges, unsigned long long* first_edge);
 /* Entries pushed from the host cache since the last init (4 bytes each crossed the link). */
 int excent_engine_host_pushed(excent_engine* e, unsigned long long* entries);
-
-/* Direction-optimised passes for the device solve on a SYMMETRIC graph (every
- * edge stored in both directions): a pass whose pending demand (sum of
- * pending degrees) is at least pull_frac * m runs as a gather. It takes every
- * pending vertex (no concurrent updates in that pass), writes its per-entry
- * weight, then adds to each vertex the weights of its neighbours: the sum the
- * scatter would have added, without atomics. 0 turns it off (the default; on
- * R-MAT graphs a gather pass is a Jacobi step and the solve pushes more entries
- * than it saves in atomics). Ignored while a host cache is set. No reference
- * counterpart: the reference always scatters. */
-int excent_engine_set_pull(excent_engine* e, double pull_frac);
 
 /* FP64 eigenvector normalisation step: with the unit principal eigenvector
  * v1 (n floats, host or device pointer; NULL turns it off), every snapshot
