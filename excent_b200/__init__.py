@@ -254,6 +254,13 @@ class Engine:
         return dict(zip(("snapshot", "plan", "push", "hub"), ms.tolist())), p.value
 
 
+def reduction_peak(n, vec4=False, ops=1 << 28, device=0):
+    """Random FP32 (or float4) reductions per second into an n-vertex array (excent_reduction_peak)."""
+    v = C.c_double()
+    call("excent_reduction_peak", int(device), int(n), int(bool(vec4)), int(ops), C.byref(v))
+    return v.value
+
+
 def ppr_fp64(n, d_idx, d_adj, seeds, values, d=0.85, tol=1e-10, maxit=2000, device=0):
     """FP64 personalized PageRank of one seed set on a device graph (excent_ppr_fp64); values is a
     scalar (the same residual at every seed) or one value per seed."""

@@ -31,7 +31,8 @@ class Measures(C.Structure):
 
 class PassLog(C.Structure):
     _fields_ = [("pending", u64), ("demand", u64), ("hot_pending", u64), ("pushed", u64),
-                ("rsum", C.c_double * 3), ("n_list", C.c_int), ("n_range", C.c_int)]
+                ("rsum", C.c_double * 3), ("n_list", C.c_int), ("n_range", C.c_int), ("lanes", u64),
+                ("taken", u64)]
 
 
 class Stats(C.Structure):
@@ -68,6 +69,7 @@ PROTOS = [
     ("excent_engine_hot_edges", C.c_int, [vp, i32p]),
     ("excent_mtx_to_egr", C.c_int, [C.c_char_p, C.c_char_p, C.c_int, u64p]),
     ("excent_engine_set_chunk_sweep", C.c_int, [vp, C.c_int]),
+    ("excent_reduction_peak", C.c_int, [C.c_int, C.c_int, C.c_int, u64, f64p]),
     ("excent_egr_report", C.c_int, [C.c_char_p, C.c_char_p, C.c_int]),
     ("excent_engine_sync", C.c_int, [vp]),
     ("excent_engine_solve", C.c_int, [vp, C.c_double, C.c_int, C.c_int]),

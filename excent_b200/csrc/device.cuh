@@ -37,6 +37,11 @@ __device__ __forceinline__ void red_add(float4* r, int u, float4 p) {
 }
 
 __device__ __forceinline__ bool nonzero(float p) { return p != 0.f; }
+// measures a push weight carries (nonzero components)
+__device__ __forceinline__ unsigned measures_in(float p) { return p != 0.f; }
+__device__ __forceinline__ unsigned measures_in(float4 p) {
+    return (unsigned)(p.x != 0.f) + (unsigned)(p.y != 0.f) + (unsigned)(p.z != 0.f);
+}
 __device__ __forceinline__ bool nonzero(float4 p) { return p.x != 0.f || p.y != 0.f || p.z != 0.f || p.w != 0.f; }
 
 __device__ __forceinline__ float shfl(float v, int src) { return __shfl_sync(FULL, v, src); }

@@ -52,10 +52,12 @@ struct Ctrl {
     double ev_corr;    // component removed from r_ev by the next snapshot
     ull host_pushed;   // entries pushed from lists read in place in host memory
     ull chunk_runs;    // chunk launches a sweeping solve ran (chunks with items, summed over passes)
+    ull lanes;         // sum over pushed lists of entries x measures carrying a nonzero weight
+    ull taken;         // sum over pushed vertices of the measures taken
 };
 
 struct PassRec {
-    ull pending, demand, hot_pending, pushed_before;
+    ull pending, demand, hot_pending, pushed_before, lanes_before, taken_before;
     double rsum[MAXM];
     int n_list, n_range;
     int pad, pad1;
@@ -66,6 +68,7 @@ struct SnapArgs {
     void* r;
     const float* v1;   // unit principal eigenvector (EV normalisation step) or null
     int ev;            // measure index of the eigenvector
+    double ev_skip;    // a pending v1 correction up to this size is carried, not written
     DevMeasures M;
     const ull* idx;
     const int* cv0;
@@ -197,7 +200,11 @@ __global__ void __launch_bounds__(BLOCK) k_snapshot(SnapArgs a) {
     long long g0 = gw * a.groups_per_warp, g1 = g0 + a.groups_per_warp;
     if (g1 > ngroups) g1 = ngroups;
     double rs0 = 0, rs1 = 0, rs2 = 0, evd = 0;
-    const double evc = a.v1 ? a.ctrl->ev_corr : 0.0;
+    // the v1 component measured by the previous snapshot is removed here only once it
+    // matters (|c| max|v1| above a thousandth of eps); until then the residuals stay as
+    // stored and the next dot product measures the component again, carried over
+    const double evc_in = a.v1 ? a.ctrl->ev_corr : 0.0;
+    const double evc = fabs(evc_in) > a.ev_skip ? evc_in : 0.0;
     unsigned hp = 0;
     for (long long g = g0; g < g1; g++) {
         const long long w0 = g * SNAP_GROUP;
@@ -385,6 +392,7 @@ __global__ void k_plan(int nc, const int* cv0, int n, ull* cnt, const uint8_t* c
         if (!stop && p < log_cap) {
             PassRec& R = log[p];
             R.pending = pend; R.demand = dem; R.hot_pending = hp; R.pushed_before = ctrl->pushed;
+            R.lanes_before = ctrl->lanes; R.taken_before = ctrl->taken;
             for (int k = 0; k < MAXM; k++) R.rsum[k] = ctrl->rsum[k];
             R.n_list = s_nl; R.n_range = s_nr;
         }
@@ -495,12 +503,12 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
     __shared__ const int* s_nb[BLOCK / 32][32];
     __shared__ unsigned s_ex[BLOCK / 32][32];
     __shared__ T s_p[BLOCK / 32][32];
-    __shared__ ull s_pushed[BLOCK / 32];
+    __shared__ ull s_pushed[3][BLOCK / 32];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     const long long first = item_first<SRC>(a), total = item_total<SRC>(a);
-    ull pushed = 0, hpushed = 0;
+    ull pushed = 0, hpushed = 0, lanes = 0, taken = 0;
     for (long long tile = gw; first + tile * 32 < total; tile += nwarps) {
         int v = 0;
         const int* nb = nullptr;
@@ -513,7 +521,10 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
             act = nonzero(p) && deg > 0;
         }
         if (act) {
+            const unsigned nz = measures_in(p);
             pushed += deg;
+            lanes += deg * nz;
+            taken += nz;
             if ((SRC == SRC_TABLE || SRC == SRC_HUBS) && a.hcache && a.idx[v] >= a.cache_edges) hpushed += deg;
         }
         const bool large = act && deg > HUB_MIN;
@@ -578,16 +589,18 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
         }
     }
     pushed = warp_sum(pushed);
-    if (lane == 0) s_pushed[wib] = pushed;
+    lanes = warp_sum(lanes);
+    taken = warp_sum(taken);
+    if (lane == 0) { s_pushed[0][wib] = pushed; s_pushed[1][wib] = lanes; s_pushed[2][wib] = taken; }
     if (a.hcache) {   // rare path (zero-copy host lists): one atomic per warp
         hpushed = warp_sum(hpushed);
         if (lane == 0 && hpushed) atomicAdd(&a.ctrl->host_pushed, hpushed);
     }
     hacc_flush(hacc, r, a.hub_id, a.hub_k);
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 3) {
         ull t = 0;
-        for (int i = 0; i < BLOCK / 32; i++) t += s_pushed[i];
-        if (t) atomicAdd(&a.ctrl->pushed, t);
+        for (int i = 0; i < BLOCK / 32; i++) t += s_pushed[threadIdx.x][i];
+        if (t) atomicAdd(threadIdx.x == 0 ? &a.ctrl->pushed : threadIdx.x == 1 ? &a.ctrl->lanes : &a.ctrl->taken, t);
     }
 }
 
@@ -766,6 +779,7 @@ struct excent_engine {
     std::vector<cudaGraphConditionalHandle> h_chunk_if;
     bool hubv_stale = true;
     bool ev_proj = false;
+    double ev_skip = 0;      // carry (do not write) a v1 correction of at most this size
     int ev_index = -1;
     int* d_cache = nullptr;
     ull cache_edges = 0;
@@ -1096,6 +1110,7 @@ static SnapArgs snap_args(excent_engine* e, bool use_hot) {
     a.r = e->d_r; a.M = e->M; a.idx = e->d_idx; a.cv0 = e->d_cv0;
     a.v1 = e->ev_proj ? e->d_v1 : nullptr;
     a.ev = e->ev_index;
+    a.ev_skip = e->ev_skip;
     a.hot = use_hot ? e->d_hot : nullptr;
     a.bitmap = e->d_bitmap; a.cnt = e->d_cnt; a.list = e->d_list;
     a.trace = e->trace_on ? e->d_trace : nullptr;
@@ -1723,6 +1738,8 @@ extern "C" int excent_engine_stats(excent_engine* e, excent_stats* st, excent_pa
             excent_pass_log& L = log[p];
             L.pending = recs[p].pending; L.demand = recs[p].demand; L.hot_pending = recs[p].hot_pending;
             L.pushed = (p + 1 < np ? recs[p + 1].pushed_before : c.pushed) - recs[p].pushed_before;
+            L.lanes = (p + 1 < np ? recs[p + 1].lanes_before : c.lanes) - recs[p].lanes_before;
+            L.taken = (p + 1 < np ? recs[p + 1].taken_before : c.taken) - recs[p].taken_before;
             for (int k = 0; k < MAXM; k++) L.rsum[k] = recs[p].rsum[k];
             L.n_list = recs[p].n_list; L.n_range = recs[p].n_range;
         }
@@ -1901,6 +1918,13 @@ extern "C" int excent_engine_ev_project(excent_engine* e, const float* d_v1) {
     EX_CHECK_ARG(ev >= 0, "the run has no eigenvector measure");
     if (!e->d_v1) EX_ALLOC(e->d_v1, (size_t)e->n * sizeof(float));
     EX_CUDA(cudaMemcpy(e->d_v1, d_v1, (size_t)e->n * sizeof(float), cudaMemcpyDefault));
+    {
+        std::vector<float> h((size_t)e->n);
+        EX_CUDA(cudaMemcpy(h.data(), e->d_v1, (size_t)e->n * sizeof(float), cudaMemcpyDeviceToHost));
+        float vmax = 0.f;
+        for (float q : h) vmax = std::max(vmax, std::fabs(q));
+        e->ev_skip = vmax > 0.f ? 1e-3 * (double)e->M.eps[ev] / (double)vmax : 0.0;
+    }
     e->ev_index = ev;
     e->ev_proj = true;
     return EXCENT_OK;

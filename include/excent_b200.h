@@ -197,6 +197,8 @@ typedef struct excent_pass_log {
     unsigned long long pushed;    /* adjacency entries pushed in the pass */
     double rsum[3];               /* FP64 sum of |r| per measure at the snapshot */
     int n_list, n_range;          /* chunks pushed as lists / whole ranges */
+    unsigned long long lanes;     /* entries pushed x measures with a nonzero weight (== pushed for one measure) */
+    unsigned long long taken;     /* measures taken over the pushed vertices (== pushed vertices for one measure) */
 } excent_pass_log;
 
 typedef struct excent_stats {
@@ -361,6 +363,12 @@ int excent_params_main(int argc, char** argv);
  * doubles) and --compare / --rank / --compare-dumps of float32 dumps against
  * it (tools/centrality_reference.cu:71-214: same modes, files and lines). */
 int excent_reference_main(int argc, char** argv);
+
+/* Measured ceiling of the scatter's operation: `ops` reductions
+ * (red.global.add.f32, or .v4.f32 with vec4) to uniformly random vertices of
+ * an n-vertex array, best of three timed launches; per_second = ops / time.
+ * Allocates the array for the call. No counterpart in the reference. */
+int excent_reduction_peak(int device, int n, int vec4, unsigned long long ops, double* per_second);
 
 /* ------------------------------------------------------------ EGR file tools */
 
