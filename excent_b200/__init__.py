@@ -212,6 +212,12 @@ class Engine:
         code = {"table": 0, "first": 1, "last": 2, False: 0, True: 1}[order]
         call("excent_engine_set_hub_order", self.h, code)
 
+    def scatter_peak(self):
+        """Entries per second of one reduction per edge-cache entry (excent_engine_scatter_peak)."""
+        v = C.c_double()
+        call("excent_engine_scatter_peak", self.h, C.byref(v))
+        return v.value
+
     def set_chunk_sweep(self, on=True):
         """Cached pushes one chunk per launch, in chunk order (the reference's launch order)."""
         call("excent_engine_set_chunk_sweep", self.h, int(bool(on)))

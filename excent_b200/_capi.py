@@ -70,6 +70,7 @@ PROTOS = [
     ("excent_mtx_to_egr", C.c_int, [C.c_char_p, C.c_char_p, C.c_int, u64p]),
     ("excent_engine_set_chunk_sweep", C.c_int, [vp, C.c_int]),
     ("excent_reduction_peak", C.c_int, [C.c_int, C.c_int, C.c_int, u64, f64p]),
+    ("excent_engine_scatter_peak", C.c_int, [vp, f64p]),
     ("excent_egr_report", C.c_int, [C.c_char_p, C.c_char_p, C.c_int]),
     ("excent_engine_sync", C.c_int, [vp]),
     ("excent_engine_solve", C.c_int, [vp, C.c_double, C.c_int, C.c_int]),

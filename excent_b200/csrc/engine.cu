@@ -32,9 +32,19 @@ enum { WT_NONE = 0, WT_LIST = 1, WT_RANGE = 2 };
 struct HubSeg {
     const int* nb;
     unsigned len;
-    unsigned pad;
+    unsigned tag;      // set to 1 once the segment is written; cleared by the warp that scatters it
     float4 p;
 };
+
+// The work queue of one push launch: tiles are claimed in batches from
+// `claim` (high 32 bits: batches claimed, low 32 bits: warps still working on
+// a batch), long lists are queued as segments at `tail` and taken from `head`
+// by warps that ran out of tiles. Zeroed before every launch.
+struct PushQueue {
+    ull tail, head, claim, pad;
+};
+static constexpr int TILE_BATCH = 8;            // tiles (of 32 items) per claim
+static constexpr unsigned SPIN_LIMIT = 1u << 24; // bounded waits for a queued segment (about a second)
 
 // Device control block: counters that live across kernels of one pass.
 struct Ctrl {
@@ -43,7 +53,7 @@ struct Ctrl {
     ull items;         // work items of the cached push in this pass
     int pass;          // passes that pushed so far
     int done;          // 1 once a snapshot found nothing pending (or max passes)
-    int err;           // nonzero: a device-side capacity check failed
+    int err;           // 1: a hub queue overflowed; 2: a bounded wait for a queued segment gave up
     int pad0;
     double rsum[MAXM]; // FP64 sum |r| of the last snapshot
     unsigned hcount;   // hot pending list length
@@ -111,7 +121,7 @@ struct PushArgs {
     // outputs
     HubSeg* hubq;
     ull hub_cap;
-    ull* hub_cnt;
+    PushQueue* q;
     Ctrl* ctrl;
     // hub-target aggregation: encoded cache entries name slots of hub_id[hub_k]
     const int* hub_id;
@@ -337,7 +347,7 @@ __global__ void __launch_bounds__(BLOCK) k_snapshot(SnapArgs a) {
 // termination (src/excent.cu:680, max passes :656), reset the counters the
 // next snapshot accumulates into, and set the graph's loop condition.
 __global__ void k_plan(int nc, const int* cv0, int n, ull* cnt, const uint8_t* cmode, double list_frac, int max_passes,
-                       uint8_t* wt_type, unsigned* wt_prefix, Ctrl* ctrl, ull* hub_cnt, PassRec* log, int log_cap,
+                       uint8_t* wt_type, unsigned* wt_prefix, Ctrl* ctrl, PushQueue* q0, PassRec* log, int log_cap,
                        cudaGraphConditionalHandle cond, int use_cond, const cudaGraphConditionalHandle* chunk_if) {
     __shared__ ull s_pend, s_dem;
     __shared__ unsigned s_carry;
@@ -399,7 +409,7 @@ __global__ void k_plan(int nc, const int* cv0, int n, ull* cnt, const uint8_t* c
         ctrl->items = stop ? 0 : s_carry;
         ctrl->chunk_runs += s_runs;
         if (stop) ctrl->done = 1; else ctrl->pass = p + 1;
-        *hub_cnt = 0;
+        q0->tail = 0; q0->head = 0; q0->claim = 0;
         ctrl->hotpend = 0;
         ctrl->ev_corr = ctrl->ev_dot;
         ctrl->ev_dot = 0;
@@ -486,6 +496,53 @@ __device__ __forceinline__ long long item_total(const PushArgs& a) {
     else return a.ctrl->hcount;
 }
 
+// A warp that ran out of tiles takes queued segments of long lists (HUB_SEG
+// entries each) one at a time and scatters them, until every batch of tiles
+// has been claimed and finished and the queue is empty. A claimed segment
+// index below the tail has been reserved by a warp that writes it without
+// waiting on anything, so the wait for its tag ends; the waits are still
+// bounded (about a second), after which ctrl->err = 2 and the warp stops.
+template <typename T>
+__device__ __forceinline__ void drain_segments(const PushArgs& a, T* r, T* hacc, int lane, long long nbatch) {
+    for (;;) {
+        ull i = 0;
+        int state = 0;   // 1 the segment is ready, 2 nothing more to do, 3 an index past the queue's capacity
+        if (lane == 0) {
+            i = atomicAdd(&a.q->head, 1ull);
+            for (unsigned it = 0;; it++) {
+                const ull tail = *(volatile ull*)&a.q->tail;
+                if (i < tail) {
+                    if (i >= a.hub_cap) { state = 3; break; }   // never written (the producer flagged it)
+                    if (*(volatile unsigned*)&a.hubq[i].tag) { state = 1; break; }
+                } else {
+                    const ull cw = *(volatile ull*)&a.q->claim;
+                    if ((long long)(cw >> 32) >= nbatch && (cw & 0xffffffffull) == 0) {
+                        __threadfence();
+                        if (i >= *(volatile ull*)&a.q->tail) { state = 2; break; }
+                        continue;   // reserved meanwhile: wait for its tag
+                    }
+                }
+                if (it >= SPIN_LIMIT) { atomicExch(&a.ctrl->err, 2); state = 2; break; }
+                __nanosleep(100);
+            }
+        }
+        state = __shfl_sync(FULL, state, 0);
+        if (state == 2) return;
+        if (state == 3) continue;
+        i = __shfl_sync(FULL, i, 0);
+        __threadfence();
+        const HubSeg* hs = a.hubq + i;
+        const int* nb = (const int*)__ldcg((const unsigned long long*)&hs->nb);
+        const unsigned len = __ldcg(&hs->len);
+        const float4 p4 = __ldcg(&hs->p);
+        __syncwarp();
+        if (lane == 0) *(volatile unsigned*)&a.hubq[i].tag = 0u;   // the slot is clean for the next launch
+        T p;
+        if constexpr (sizeof(T) == sizeof(float)) p = p4.x; else p = p4;
+        warp_scatter(r, nb, len, p, lane, hacc);
+    }
+}
+
 // Push kernel (persistent grid, warp tiles of 32 items). Each lane takes one
 // item's residual (the push-time re-check and exchange of
 // src/excent.cu:109-112), then the warp dispatches by degree: lists of up to
@@ -505,11 +562,17 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
     __shared__ T s_p[BLOCK / 32][32];
     __shared__ ull s_pushed[3][BLOCK / 32];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     const long long first = item_first<SRC>(a), total = item_total<SRC>(a);
+    const long long ntiles = total > first ? (total - first + 31) / 32 : 0;
+    const long long nbatch = (ntiles + TILE_BATCH - 1) / TILE_BATCH;
     ull pushed = 0, hpushed = 0, lanes = 0, taken = 0;
-    for (long long tile = gw; first + tile * 32 < total; tile += nwarps) {
+    for (;;) {
+    // claim the next batch of tiles (and count this warp as working on it)
+    ull claim = 0;
+    if (lane == 0) claim = atomicAdd(&a.q->claim, (1ull << 32) | 1ull);
+    const long long batch = (long long)(__shfl_sync(FULL, claim, 0) >> 32);
+    const long long tile_end = batch < nbatch ? min((batch + 1) * TILE_BATCH, ntiles) : 0;
+    for (long long tile = batch * TILE_BATCH; tile < tile_end; tile++) {
         int v = 0;
         const int* nb = nullptr;
         ull deg = 0;
@@ -534,7 +597,7 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
         const unsigned stot = __shfl_sync(FULL, sincl, 31);
         ull sbase = 0;
         if (stot) {
-            if (lane == 0) sbase = atomicAdd(a.hub_cnt, (ull)stot);
+            if (lane == 0) sbase = atomicAdd(&a.q->tail, (ull)stot);
             sbase = __shfl_sync(FULL, sbase, 0);
         }
         if (large) {
@@ -545,10 +608,12 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
                     HubSeg h;
                     h.nb = nb + (ull)s * HUB_SEG;
                     h.len = (unsigned)min((ull)HUB_SEG, deg - (ull)s * HUB_SEG);
-                    h.pad = 0;
+                    h.tag = 0;
                     if constexpr (L == 1) h.p = make_float4(p, 0.f, 0.f, 0.f); else h.p = p;
                     q[s] = h;
                 }
+                __threadfence();   // the segments are visible before they are marked written
+                for (unsigned s = 0; s < nseg; s++) *(volatile unsigned*)&q[s].tag = 1u;
             } else {
                 atomicExch(&a.ctrl->err, 1);
             }
@@ -588,6 +653,14 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
             __syncwarp();
         }
     }
+    // done with the batch: its segments are reserved (and written) before the release
+    __syncwarp();
+    __threadfence();
+    if (lane == 0) atomicAdd(&a.q->claim, ~0ull);
+    if (batch >= nbatch) break;
+    }
+    // out of tiles: scatter queued long-list segments until none is left or coming
+    drain_segments<T>(a, r, hacc, lane, nbatch);
     pushed = warp_sum(pushed);
     lanes = warp_sum(lanes);
     taken = warp_sum(taken);
@@ -602,27 +675,6 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
         for (int i = 0; i < BLOCK / 32; i++) t += s_pushed[threadIdx.x][i];
         if (t) atomicAdd(threadIdx.x == 0 ? &a.ctrl->pushed : threadIdx.x == 1 ? &a.ctrl->lanes : &a.ctrl->taken, t);
     }
-}
-
-// Hub segments queued by k_push: one warp per HUB_SEG-entry segment.
-template <int L>
-__global__ void __launch_bounds__(BLOCK) k_hub(void* rv, const HubSeg* q, const ull* hub_cnt, ull cap,
-                                               const int* hub_id, int hub_k) {
-    typedef typename Lane<L>::T T;
-    T* r = reinterpret_cast<T*>(rv);
-    T* hacc = hacc_init<T>(hub_k);
-    const int lane = threadIdx.x & 31;
-    const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    ull cnt = *hub_cnt;
-    if (cnt > cap) cnt = cap;
-    for (long long s = gw; s < (long long)cnt; s += nwarps) {
-        const HubSeg h = q[s];
-        T p;
-        if constexpr (L == 1) p = h.p.x; else p = h.p;
-        warp_scatter(r, h.nb, h.len, p, lane, hacc);
-    }
-    hacc_flush(hacc, r, hub_id, hub_k);
 }
 
 // Pending hot vertices among hot ids [lo, hi) at launch time, appended with
@@ -758,7 +810,7 @@ struct excent_engine {
     unsigned* d_wt_prefix = nullptr;
     HubSeg* d_hubq[3] = {nullptr, nullptr, nullptr};  // per stream: main, slot 0, slot 1
     ull hub_cap[3] = {0, 0, 0};
-    ull* d_hubcnt = nullptr;                           // 3 counters
+    PushQueue* d_queue = nullptr;                      // per stream: main, slot 0, slot 1
     bool hot_skip = false;                             // this pass skips cached high-degree vertices
     PassRec* d_log = nullptr;
     int log_cap = 0;
@@ -821,6 +873,8 @@ static void invalidate_graph(excent_engine* e) {
     if (e->graph) { cudaGraphDestroy(e->graph); e->graph = nullptr; }
 }
 
+static void scrub_queues(excent_engine* e);
+
 static int free_engine(excent_engine* e) {
     if (!e) return EXCENT_OK;
     cudaSetDevice(e->dev);
@@ -828,7 +882,7 @@ static int free_engine(excent_engine* e) {
     if (e->gexec) cudaGraphExecDestroy(e->gexec);
     if (e->graph) cudaGraphDestroy(e->graph);
     void* dptrs[] = {e->d_chunk_if, e->d_hub_id, e->d_hubv, e->d_hubv_cnt, e->d_v1, e->d_idx, e->d_x, e->d_r, e->d_bitmap, e->d_cnt, e->d_cv0, e->d_list, e->d_ctrl, e->d_cmode,
-                     e->d_wt_type, e->d_wt_prefix, e->d_hubq[0], e->d_hubq[1], e->d_hubq[2], e->d_hubcnt, e->d_log, e->d_trace, e->d_tmp, e->d_cache,
+                     e->d_wt_type, e->d_wt_prefix, e->d_hubq[0], e->d_hubq[1], e->d_hubq[2], e->d_queue, e->d_log, e->d_trace, e->d_tmp, e->d_cache,
                      e->d_hids, e->d_hoff, e->d_hedges, e->d_hot, e->d_hlist};
     for (void* p : dptrs) if (p) cudaFree(p);
     void* hptrs[] = {e->h_cnt, e->h_ctrl, e->h_wt_type, e->h_wt_prefix};
@@ -898,7 +952,7 @@ static int engine_setup(excent_engine* e, int device, int n, ull m, const excent
     EX_ALLOC(e->d_wt_prefix, ((size_t)nc + 1) * sizeof(unsigned));
     e->hub_cap[0] = m / HUB_SEG + m / HUB_MIN + 64;
     EX_ALLOC(e->d_hubq[0], e->hub_cap[0] * sizeof(HubSeg));
-    EX_ALLOC(e->d_hubcnt, 3 * sizeof(ull));
+    EX_ALLOC(e->d_queue, 3 * sizeof(PushQueue));
     e->log_cap = 1 << 17;
     EX_ALLOC(e->d_log, (size_t)e->log_cap * sizeof(PassRec));
     if (e->L == 4) EX_ALLOC(e->d_tmp, (size_t)n * sizeof(float));
@@ -910,7 +964,8 @@ static int engine_setup(excent_engine* e, int device, int n, ull m, const excent
     EX_CUDA(cudaMemset(e->d_ctrl, 0, sizeof(Ctrl)));
     EX_CUDA(cudaMemset(e->d_cnt, 0, 2 * (size_t)nc * sizeof(ull)));
     EX_CUDA(cudaMemset(e->d_cmode, 0, (size_t)nc));
-    EX_CUDA(cudaMemset(e->d_hubcnt, 0, 3 * sizeof(ull)));
+    EX_CUDA(cudaMemset(e->d_queue, 0, 3 * sizeof(PushQueue)));
+    EX_CUDA(cudaMemset(e->d_hubq[0], 0, e->hub_cap[0] * sizeof(HubSeg)));   // every tag clear
     int occ = 0;
     if (e->L == 1) EX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_push<1, SRC_TABLE>, BLOCK, 0));
     else EX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_push<4, SRC_TABLE>, BLOCK, 0));
@@ -1071,7 +1126,7 @@ extern "C" int excent_engine_read_trace(excent_engine* e, uint16_t* out) {
 
 static int reset_counters(excent_engine* e) {
     EX_CUDA(cudaMemsetAsync(e->d_ctrl, 0, sizeof(Ctrl), e->s_main));
-    EX_CUDA(cudaMemsetAsync(e->d_hubcnt, 0, 3 * sizeof(ull), e->s_main));
+    EX_CUDA(cudaMemsetAsync(e->d_queue, 0, 3 * sizeof(PushQueue), e->s_main));
     EX_CUDA(cudaMemsetAsync(e->d_cnt, 0, 2 * (size_t)e->nc * sizeof(ull), e->s_main));
     if (e->d_trace && e->trace_on) EX_CUDA(cudaMemsetAsync(e->d_trace, 0, (size_t)e->n * sizeof(uint16_t), e->s_main));
     e->hot_skip = false;
@@ -1177,7 +1232,7 @@ static PushArgs push_args(excent_engine* e, int q) {
     a.nc = e->nc; a.cv0 = e->d_cv0; a.wt_type = e->d_wt_type; a.wt_prefix = e->d_wt_prefix; a.list = e->d_list;
     a.cache = e->d_cache;
     a.hids = e->d_hids; a.hoff = e->d_hoff; a.hedges = e->d_hedges; a.hlist = e->d_hlist;
-    a.hubq = e->d_hubq[q]; a.hub_cap = e->hub_cap[q]; a.hub_cnt = e->d_hubcnt + q; a.ctrl = e->d_ctrl;
+    a.hubq = e->d_hubq[q]; a.hub_cap = e->hub_cap[q]; a.q = e->d_queue + q; a.ctrl = e->d_ctrl;
     a.hub_id = e->d_hub_id; a.hub_k = e->hub_k;
     a.hubv = e->d_hubv; a.hubv_cnt = e->d_hubv_cnt; a.skip_hubs = 0; a.chunk = -1;
     a.hcache = nullptr; a.cache_edges = e->cache_edges;
@@ -1185,16 +1240,14 @@ static PushArgs push_args(excent_engine* e, int q) {
     return a;
 }
 
+// One push launch: its work queue zeroed, then the kernel (which scatters its
+// own long-list segments).
 template <int SRC>
 static void launch_push(excent_engine* e, const PushArgs& a, int grid, cudaStream_t st) {
-    if (e->L == 1) {
-        k_push<1, SRC><<<grid, BLOCK, hub_smem(e), st>>>(a);
-        k_hub<1><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
-    } else {
-        k_push<4, SRC><<<grid, BLOCK, hub_smem(e), st>>>(a);
-        k_hub<4><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
-    }
-    e->launches += 2;
+    cudaMemsetAsync(a.q, 0, sizeof(PushQueue), st);
+    if (e->L == 1) k_push<1, SRC><<<grid, BLOCK, hub_smem(e), st>>>(a);
+    else k_push<4, SRC><<<grid, BLOCK, hub_smem(e), st>>>(a);
+    e->launches++;
 }
 
 static int grid_for(excent_engine* e, ull items) {
@@ -1227,7 +1280,6 @@ extern "C" int excent_engine_push_cached(excent_engine* e, const unsigned char* 
     EX_CUDA(cudaMemcpyAsync(e->d_wt_type, e->h_wt_type, e->nc, cudaMemcpyHostToDevice, e->s_main));
     EX_CUDA(cudaMemcpyAsync(e->d_wt_prefix, e->h_wt_prefix, ((size_t)e->nc + 1) * sizeof(unsigned),
                             cudaMemcpyHostToDevice, e->s_main));
-    EX_CUDA(cudaMemsetAsync(e->d_hubcnt, 0, sizeof(ull), e->s_main));
     PushArgs a = push_args(e, 0);
     a.hot = e->hot_skip ? e->d_hot : nullptr;
     if (e->chunk_sweep) {   // one launch (and its hub segments) per chunk, in chunk order
@@ -1235,7 +1287,6 @@ extern "C" int excent_engine_push_cached(excent_engine* e, const unsigned char* 
             const unsigned items = e->h_wt_prefix[c + 1] - e->h_wt_prefix[c];
             if (!items) continue;
             a.chunk = c;
-            if (c) EX_CUDA(cudaMemsetAsync(e->d_hubcnt, 0, sizeof(ull), e->s_main));
             launch_push<SRC_TABLE>(e, a, grid_for(e, items), e->s_main);
         }
     } else {
@@ -1279,6 +1330,7 @@ extern "C" int excent_engine_slots_create(excent_engine* e, unsigned long long m
         const ull me = std::max<ull>(max_chunk_edges, 1);
         e->hub_cap[q] = me / HUB_SEG + me / HUB_MIN + 64;
         EX_ALLOC(e->d_hubq[q], e->hub_cap[q] * sizeof(HubSeg));
+        EX_CUDA(cudaMemset(e->d_hubq[q], 0, e->hub_cap[q] * sizeof(HubSeg)));
     }
     e->max_chunk_edges = std::max<ull>(e->max_chunk_edges, max_chunk_edges);
     e->slots_ok = true;
@@ -1327,7 +1379,6 @@ extern "C" int excent_engine_push_stream(excent_engine* e, int s, int c, const u
     a.cv_0 = v0; a.ebase = dst; a.e0 = e0;
     if ((double)k < list_frac * nv) { a.ctype = WT_LIST; a.ccount = (unsigned)k; e->n_list++; }
     else { a.ctype = WT_RANGE; a.ccount = (unsigned)nv; e->n_range++; }
-    EX_CUDA(cudaMemsetAsync(e->d_hubcnt + 1 + s, 0, sizeof(ull), sl.st));
     if (a.ccount) launch_push<SRC_CHUNK>(e, a, grid_for(e, a.ccount), sl.st);
     EX_CUDA(cudaGetLastError());
     if (to_cache) e->loaded[c] = 1;
@@ -1349,7 +1400,6 @@ extern "C" int excent_engine_push_gather(excent_engine* e, int s, int k, unsigne
     if (k) {
         PushArgs a = push_args(e, 1 + s);
         a.vids = sl.d_vids; a.off = sl.d_off; a.gedges = sl.d_edges; a.gk = (unsigned)k;
-        EX_CUDA(cudaMemsetAsync(e->d_hubcnt + 1 + s, 0, sizeof(ull), sl.st));
         launch_push<SRC_GATHER>(e, a, grid_for(e, (ull)k), sl.st);
         EX_CUDA(cudaGetLastError());
     }
@@ -1398,7 +1448,6 @@ extern "C" int excent_engine_push_hot(excent_engine* e, int lo, int hi, int afte
     if (e->L == 1) k_compact_hot<1><<<grid, BLOCK, 0, e->s_main>>>(lo, hi, e->d_hids, e->d_r, e->M, e->d_hlist, e->d_ctrl);
     else k_compact_hot<4><<<grid, BLOCK, 0, e->s_main>>>(lo, hi, e->d_hids, e->d_r, e->M, e->d_hlist, e->d_ctrl);
     e->launches++;
-    EX_CUDA(cudaMemsetAsync(e->d_hubcnt, 0, sizeof(ull), e->s_main));
     PushArgs a = push_args(e, 0);
     launch_push<SRC_HOT>(e, a, grid_for(e, (ull)(hi - lo)), e->s_main);
     EX_CUDA(cudaGetLastError());
@@ -1442,7 +1491,9 @@ extern "C" int excent_engine_sync(excent_engine* e) {
     if (e->slots_ok) for (Slot& s : e->slot) { EX_CUDA(cudaStreamSynchronize(s.st)); s.busy = false; }
     int err = 0;
     EX_CUDA(cudaMemcpy(&err, &e->d_ctrl->err, sizeof(int), cudaMemcpyDeviceToHost));
-    if (err) EX_FAIL(EXCENT_ERR_STATE, "device capacity check failed (hub queue overflow)");
+    if (err) scrub_queues(e);
+    if (err) EX_FAIL(EXCENT_ERR_STATE, "%s", err == 2 ? "a push kernel's wait for a queued segment timed out"
+                                                  : "device capacity check failed (hub queue overflow)");
     return EXCENT_OK;
 }
 
@@ -1479,8 +1530,8 @@ static cudaError_t close_if(cudaStream_t body) {
 // Kernels of one pass outside the per-chunk launches of a chunk sweep, and per
 // chunk launch (for the launch count of a graph solve).
 static void pass_kernels(const excent_engine* e, int order, ull* fixed, ull* per_chunk) {
-    *fixed = 2 + (order == 1 || order == 2 ? 2 : 0) + (e->chunk_sweep ? 0 : (order == 0 ? 2 : 1));
-    *per_chunk = e->chunk_sweep ? (order == 0 ? 2 : 1) : 0;
+    *fixed = 2 + (order == 1 || order == 2 ? 1 : 0) + (e->chunk_sweep ? 0 : 1);
+    *per_chunk = e->chunk_sweep ? 1 : 0;
 }
 
 static int effective_order(const excent_engine* e) {
@@ -1500,7 +1551,7 @@ static cudaError_t enqueue_pass(excent_engine* e, double list_frac, int max_pass
     if (ev) cudaEventRecord(ev[1], st);
     const bool use_if = chunk_body && e->chunk_sweep;
     k_plan<<<1, 1024, 0, st>>>(e->nc, e->d_cv0, e->n, e->d_cnt, e->d_cmode, list_frac, max_passes, e->d_wt_type,
-                               e->d_wt_prefix, e->d_ctrl, e->d_hubcnt, e->d_log, e->log_cap, cond, use_cond,
+                               e->d_wt_prefix, e->d_ctrl, e->d_queue, e->d_log, e->log_cap, cond, use_cond,
                                use_if ? e->d_chunk_if : nullptr);
     e->launches++;
     if (ev) cudaEventRecord(ev[2], st);
@@ -1509,31 +1560,23 @@ static cudaError_t enqueue_pass(excent_engine* e, double list_frac, int max_pass
     // pass's residual reaches every other vertex before that vertex is taken; 2 = last, so they
     // collect the pass's residual and push it once; 0 = in table order with the rest
     const int order = effective_order(e);
-    auto hubs = [&](cudaStream_t s) {
-        if (e->L == 1) k_hub<1><<<e->grid_push, BLOCK, hub_smem(e), s>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
-        else k_hub<4><<<e->grid_push, BLOCK, hub_smem(e), s>>>(e->d_r, a.hubq, a.hub_cnt, a.hub_cap, e->d_hub_id, e->hub_k);
-        e->launches++;
-    };
     auto table = [&](cudaStream_t s) {
+        cudaMemsetAsync(a.q, 0, sizeof(PushQueue), s);
         if (e->L == 1) k_push<1, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), s>>>(a);
         else k_push<4, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), s>>>(a);
         e->launches++;
     };
     auto hub_phase = [&]() {
-        // every list of SRC_HUBS is longer than HUB_MIN, so this push only takes and queues:
-        // no entry is scattered here and the hub-target slots are not needed
-        PushArgs ah = a;
-        ah.hub_k = 0;
-        if (e->L == 1) k_push<1, SRC_HUBS><<<e->grid_push, BLOCK, 0, st>>>(ah);
-        else k_push<4, SRC_HUBS><<<e->grid_push, BLOCK, 0, st>>>(ah);
+        cudaMemsetAsync(a.q, 0, sizeof(PushQueue), st);
+        if (e->L == 1) k_push<1, SRC_HUBS><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
+        else k_push<4, SRC_HUBS><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
         e->launches++;
-        hubs(st);
     };
     if (order == 1) hub_phase();
     a.skip_hubs = order != 0;   // the table push skips the high-degree vertices
     if (e->chunk_sweep) {
-        // chunk by chunk: each chunk's push (and, in table order, its hub segments) completes
-        // before the next chunk's vertices are taken, so they see everything pushed so far
+        // chunk by chunk: each chunk's push (with its long lists) completes before the next
+        // chunk's vertices are taken, so they see everything pushed so far
         for (int c = 0; c < e->nc; c++) {
             a.chunk = c;
             cudaStream_t s = st;
@@ -1543,10 +1586,6 @@ static cudaError_t enqueue_pass(excent_engine* e, double list_frac, int max_pass
                 s = chunk_body;
             }
             table(s);
-            if (order == 0) {
-                hubs(s);
-                cudaMemsetAsync(a.hub_cnt, 0, sizeof(ull), s);
-            }
             if (use_if) {
                 const cudaError_t rc = close_if(chunk_body);
                 if (rc != cudaSuccess) return rc;
@@ -1556,8 +1595,8 @@ static cudaError_t enqueue_pass(excent_engine* e, double list_frac, int max_pass
     } else {
         table(st);
     }
+    a.skip_hubs = 0;
     if (ev) cudaEventRecord(ev[3], st);
-    if (order == 0 && !e->chunk_sweep) hubs(st);   // the table push's own segments
     if (order == 2) hub_phase();
     if (ev) cudaEventRecord(ev[4], st);
     return cudaGetLastError();
@@ -1606,6 +1645,17 @@ static int build_graph(excent_engine* e, double list_frac, int max_passes) {
     e->graph_max_passes = max_passes;
     e->graph_list_frac = list_frac;
     return EXCENT_OK;
+}
+
+// After a device-side failure, a segment may have been left marked written:
+// clear every queue and tag (and the flag) so no later launch reads one.
+static void scrub_queues(excent_engine* e) {
+    cudaDeviceSynchronize();
+    for (int q = 0; q < 3; q++)
+        if (e->d_hubq[q]) cudaMemset(e->d_hubq[q], 0, e->hub_cap[q] * sizeof(HubSeg));
+    cudaMemset(e->d_queue, 0, 3 * sizeof(PushQueue));
+    cudaMemset(&e->d_ctrl->err, 0, sizeof(int));
+    cudaDeviceSynchronize();
 }
 
 static int solve_impl(excent_engine* e, double list_frac, int max_passes, int use_graph, bool init);
@@ -1710,7 +1760,9 @@ static int solve_impl(excent_engine* e, double list_frac, int max_passes, int us
         }
     }
     EX_CUDA(cudaGetLastError());
-    if (e->h_ctrl->err) EX_FAIL(EXCENT_ERR_STATE, "device capacity check failed (hub queue overflow)");
+    if (e->h_ctrl->err) scrub_queues(e);
+    if (e->h_ctrl->err) EX_FAIL(EXCENT_ERR_STATE, "%s", e->h_ctrl->err == 2 ? "a push kernel's wait for a queued segment timed out"
+                                                                        : "device capacity check failed (hub queue overflow)");
     return EXCENT_OK;
 }
 
@@ -1854,8 +1906,7 @@ extern "C" int excent_engine_set_hub_targets(excent_engine* e, int k) {
         cudaFuncSetAttribute(k_push<4, SRC_GATHER>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz);
         cudaFuncSetAttribute(k_push<4, SRC_HOT>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz);
         cudaFuncSetAttribute(k_push<4, SRC_HUBS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz);
-        cudaFuncSetAttribute(k_hub<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz);
-        EX_CUDA(cudaFuncSetAttribute(k_hub<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+        EX_CUDA(cudaGetLastError());
     }
     int occ = 0;
     if (e->L == 1) EX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_push<1, SRC_TABLE>, BLOCK, smem));
@@ -1869,6 +1920,56 @@ extern "C" int excent_engine_set_hub_order(excent_engine* e, int order) {
     EX_CUDA(cudaSetDevice(e->dev));
     invalidate_graph(e);
     e->hub_order = order;
+    return EXCENT_OK;
+}
+
+// Every entry of the edge cache, in cache order, reduced into a scratch array
+// shaped like r: the scatter's ceiling on this graph's target distribution.
+template <int L>
+__global__ void k_scatter_probe(ull m, const int* cache, const int* hub_id, typename Lane<L>::T* out) {
+    typedef typename Lane<L>::T T;
+    T one;
+    if constexpr (L == 1) one = 1.f; else one = make_float4(1.f, 1.f, 1.f, 0.f);
+    const ull stride = (ull)gridDim.x * blockDim.x;
+    const ull m4 = m / 4;
+    const int4* c4 = reinterpret_cast<const int4*>(cache);
+    auto dec = [&](int u) { return u < 0 ? hub_id[u & HUB_MASK] : u; };
+    for (ull i = blockIdx.x * (ull)blockDim.x + threadIdx.x; i < m4; i += stride) {
+        const int4 q = ld_edge4(c4 + i);
+        red_add(out, dec(q.x), one); red_add(out, dec(q.y), one);
+        red_add(out, dec(q.z), one); red_add(out, dec(q.w), one);
+    }
+    for (ull i = m4 * 4 + blockIdx.x * (ull)blockDim.x + threadIdx.x; i < m; i += stride) red_add(out, dec(cache[i]), one);
+}
+
+extern "C" int excent_engine_scatter_peak(excent_engine* e, double* entries_per_second) {
+    EX_CHECK_ARG(e && entries_per_second, "null argument");
+    EX_CHECK_ARG(e->d_cache && e->cache_edges == e->m, "the scatter probe needs the whole graph in the edge cache");
+    EX_CUDA(cudaSetDevice(e->dev));
+    EX_CUDA(cudaDeviceSynchronize());
+    const size_t bytes = (size_t)e->n * (e->L == 1 ? sizeof(float) : sizeof(float4));
+    void* out = nullptr;
+    if (cudaMalloc(&out, bytes) != cudaSuccess) { cudaGetLastError(); EX_FAIL(EXCENT_ERR_NOMEM, "probe array of %zu bytes", bytes); }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 0.f;
+    for (int rep = 0; rep < 4; rep++) {   // the first launch warms up; best of the other three
+        cudaEventRecord(e0, e->s_main);
+        if (e->L == 1) k_scatter_probe<1><<<e->sms * 8, BLOCK, 0, e->s_main>>>(e->m, e->d_cache, e->d_hub_id, (float*)out);
+        else k_scatter_probe<4><<<e->sms * 8, BLOCK, 0, e->s_main>>>(e->m, e->d_cache, e->d_hub_id, (float4*)out);
+        cudaEventRecord(e1, e->s_main);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0 && (best == 0.f || ms < best)) best = ms;
+    }
+    const cudaError_t rc = cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    EX_CUDA(rc);
+    *entries_per_second = best > 0.f ? (double)e->m / (best * 1e-3) : 0.0;
     return EXCENT_OK;
 }
 

@@ -247,6 +247,11 @@ int excent_engine_set_hub_order(excent_engine* e, int order);
  * previous one, as the reference launches its resident chunks on one stream,
  * src/excent.cu:684-688), or every chunk in one launch (off, the default). */
 int excent_engine_set_chunk_sweep(excent_engine* e, int on);
+/* The scatter's ceiling on this graph: one reduction per edge-cache entry (in
+ * cache order, to its target, into a scratch array shaped like the residuals),
+ * best of three timed passes, as entries per second. Needs the whole graph in
+ * the edge cache. No counterpart in the reference. */
+int excent_engine_scatter_peak(excent_engine* e, double* entries_per_second);
 
 /* Host cache for graphs larger than device memory: pinned, device-mapped host
  * memory for the entries past the HBM edge cache (entries [*first_edge, m),
