@@ -212,6 +212,18 @@ class Engine:
         code = {"table": 0, "first": 1, "last": 2, False: 0, True: 1}[order]
         call("excent_engine_set_hub_order", self.h, code)
 
+    def autotune(self, list_frac=0.5, max_passes=100000):
+        """Time the candidate settings (excent_engine_autotune), keep the fastest; returns
+        (best, [every candidate]) as dicts."""
+        best = _capi.Tune()
+        tried = (_capi.Tune * 16)()
+        nt = C.c_int()
+        call("excent_engine_autotune", self.h, float(list_frac), int(max_passes), C.byref(best), tried, 16,
+             C.byref(nt))
+        as_dict = lambda t: {"hub_targets": t.hub_targets, "hub_order": ["table", "first", "last"][t.hub_order],  # noqa: E731
+                             "chunk_sweep": bool(t.chunk_sweep), "ms": round(t.ms, 3)}
+        return as_dict(best), [as_dict(tried[i]) for i in range(nt.value)]
+
     def scatter_peak(self):
         """Entries per second of one reduction per edge-cache entry (excent_engine_scatter_peak)."""
         v = C.c_double()

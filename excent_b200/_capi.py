@@ -35,6 +35,10 @@ class PassLog(C.Structure):
                 ("taken", u64)]
 
 
+class Tune(C.Structure):
+    _fields_ = [("hub_targets", C.c_int), ("hub_order", C.c_int), ("chunk_sweep", C.c_int), ("ms", C.c_double)]
+
+
 class Stats(C.Structure):
     _fields_ = [("passes", C.c_int), ("pushed", u64), ("n_list", u64), ("n_range", u64), ("rsum", C.c_double * 3)]
 
@@ -71,6 +75,8 @@ PROTOS = [
     ("excent_engine_set_chunk_sweep", C.c_int, [vp, C.c_int]),
     ("excent_reduction_peak", C.c_int, [C.c_int, C.c_int, C.c_int, u64, f64p]),
     ("excent_engine_scatter_peak", C.c_int, [vp, f64p]),
+    ("excent_engine_autotune", C.c_int, [vp, C.c_double, C.c_int, C.POINTER(Tune), C.POINTER(Tune), C.c_int,
+                                         C.POINTER(C.c_int)]),
     ("excent_egr_report", C.c_int, [C.c_char_p, C.c_char_p, C.c_int]),
     ("excent_engine_sync", C.c_int, [vp]),
     ("excent_engine_solve", C.c_int, [vp, C.c_double, C.c_int, C.c_int]),

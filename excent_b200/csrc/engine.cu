@@ -43,7 +43,7 @@ struct HubSeg {
 struct PushQueue {
     ull tail, head, claim, pad;
 };
-static constexpr int TILE_BATCH = 8;            // tiles (of 32 items) per claim
+static constexpr int TILE_BATCH = 8;            // at most this many tiles (of 32 items) per claim
 static constexpr unsigned SPIN_LIMIT = 1u << 24; // bounded waits for a queued segment (about a second)
 
 // Device control block: counters that live across kernels of one pass.
@@ -564,15 +564,18 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const long long first = item_first<SRC>(a), total = item_total<SRC>(a);
     const long long ntiles = total > first ? (total - first + 31) / 32 : 0;
-    const long long nbatch = (ntiles + TILE_BATCH - 1) / TILE_BATCH;
+    // claims of up to TILE_BATCH tiles, fewer when there are not two claims per warp
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const long long per_claim = max(1ll, min((long long)TILE_BATCH, ntiles / (2 * nwarps)));
+    const long long nbatch = (ntiles + per_claim - 1) / per_claim;
     ull pushed = 0, hpushed = 0, lanes = 0, taken = 0;
     for (;;) {
     // claim the next batch of tiles (and count this warp as working on it)
     ull claim = 0;
     if (lane == 0) claim = atomicAdd(&a.q->claim, (1ull << 32) | 1ull);
     const long long batch = (long long)(__shfl_sync(FULL, claim, 0) >> 32);
-    const long long tile_end = batch < nbatch ? min((batch + 1) * TILE_BATCH, ntiles) : 0;
-    for (long long tile = batch * TILE_BATCH; tile < tile_end; tile++) {
+    const long long tile_end = batch < nbatch ? min((batch + 1) * per_claim, ntiles) : 0;
+    for (long long tile = batch * per_claim; tile < tile_end; tile++) {
         int v = 0;
         const int* nb = nullptr;
         ull deg = 0;
@@ -1970,6 +1973,53 @@ extern "C" int excent_engine_scatter_peak(excent_engine* e, double* entries_per_
     cudaFree(out);
     EX_CUDA(rc);
     *entries_per_second = best > 0.f ? (double)e->m / (best * 1e-3) : 0.0;
+    return EXCENT_OK;
+}
+
+// Setting candidates of the device solve, timed one full solve each on this
+// graph (after one untimed solve that builds the graph); the fastest is kept.
+extern "C" int excent_engine_autotune(excent_engine* e, double list_frac, int max_passes, excent_tune* best,
+                                      excent_tune* tried, int cap, int* ntried) {
+    EX_CHECK_ARG(e && best, "null argument");
+    EX_CHECK_ARG(e->d_cache && e->cache_edges == e->m, "autotuning needs the whole graph in the edge cache");
+    EX_CUDA(cudaSetDevice(e->dev));
+    const int k_hi = std::min(e->n, e->L == 1 ? 16384 : 4096), k_lo = std::min(e->n, e->L == 1 ? 4096 : 2048);
+    const excent_tune cands[] = {
+        {k_hi, 0, 1, 0.0}, {k_lo, 0, 1, 0.0}, {0, 0, 1, 0.0},   // table order, chunk by chunk
+        {k_hi, 1, 0, 0.0}, {k_lo, 1, 0, 0.0}, {0, 1, 0, 0.0},   // high-degree lists first, one launch
+    };
+    const int nc = (int)(sizeof cands / sizeof cands[0]);
+    cudaEvent_t t0, t1;
+    EX_CUDA(cudaEventCreate(&t0));
+    EX_CUDA(cudaEventCreate(&t1));
+    excent_tune win{};
+    win.ms = -1;
+    int rc = EXCENT_OK;
+    for (int i = 0; i < nc && rc == EXCENT_OK; i++) {
+        excent_tune c = cands[i];
+        rc = excent_engine_set_hub_targets(e, c.hub_targets);
+        if (rc == EXCENT_OK) rc = excent_engine_set_hub_order(e, c.hub_order);
+        if (rc == EXCENT_OK) rc = excent_engine_set_chunk_sweep(e, c.chunk_sweep);
+        if (rc == EXCENT_OK) rc = excent_engine_solve(e, list_frac, max_passes, 1);   // builds the graph
+        if (rc != EXCENT_OK) break;
+        cudaEventRecord(t0, e->s_main);
+        rc = excent_engine_solve(e, list_frac, max_passes, 1);
+        cudaEventRecord(t1, e->s_main);
+        cudaEventSynchronize(t1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, t0, t1);
+        c.ms = ms;
+        if (tried && i < cap) tried[i] = c;
+        if (ntried) *ntried = i + 1;
+        if (win.ms < 0 || c.ms < win.ms) win = c;
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    EX_TRY(rc);
+    EX_TRY(excent_engine_set_hub_targets(e, win.hub_targets));
+    EX_TRY(excent_engine_set_hub_order(e, win.hub_order));
+    EX_TRY(excent_engine_set_chunk_sweep(e, win.chunk_sweep));
+    *best = win;
     return EXCENT_OK;
 }
 

@@ -252,6 +252,20 @@ int excent_engine_set_chunk_sweep(excent_engine* e, int on);
  * best of three timed passes, as entries per second. Needs the whole graph in
  * the edge cache. No counterpart in the reference. */
 int excent_engine_scatter_peak(excent_engine* e, double* entries_per_second);
+/* Settings of the device solve tried by excent_engine_autotune. */
+typedef struct excent_tune {
+    int hub_targets;   /* shared-memory slots for the highest-degree targets */
+    int hub_order;     /* 0 table order, 1 high-degree lists first, 2 last */
+    int chunk_sweep;   /* 1: one launch per chunk, in chunk order */
+    double ms;         /* one solve (graph launch) with these settings */
+} excent_tune;
+/* Time one device solve for each candidate (table order chunk by chunk, or
+ * the high-degree lists first in one launch; each with 0 or two sizes of
+ * hub-target slots), keep the fastest and return it; tried (cap entries, may
+ * be NULL) receives every candidate's time. Needs the whole graph in the edge
+ * cache. No counterpart in the reference. */
+int excent_engine_autotune(excent_engine* e, double list_frac, int max_passes, excent_tune* best,
+                           excent_tune* tried, int cap, int* ntried);
 
 /* Host cache for graphs larger than device memory: pinned, device-mapped host
  * memory for the entries past the HBM edge cache (entries [*first_edge, m),
