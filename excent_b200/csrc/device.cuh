@@ -170,4 +170,39 @@ __device__ __forceinline__ void warp_scatter(P* r, const int* nb, unsigned deg, 
     if (lane < (int)tail) scatter_one(r, ld_edge(nb + head + nbody * 4 + lane), p, hacc);
 }
 
+// ---- bulk-copy staging (cp.async.bulk with an mbarrier, one per warp) ----
+// Plain, non-multicast bulk copies from this GPU's own memory into the CTA's
+// shared memory: 16-byte aligned source, destination and size.
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void bar_init(unsigned long long* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// Lane 0: expect `bytes` on the barrier and start the copy global -> shared.
+__device__ __forceinline__ void bulk_stage(unsigned long long* bar, void* dst, const void* src, unsigned bytes) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // earlier reads of dst come first
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+// Wait for the phase `parity` of the barrier to complete, at most `limit`
+// polls; false if it did not.
+__device__ __forceinline__ bool bar_wait(unsigned long long* bar, unsigned parity, unsigned limit) {
+    for (unsigned it = 0; it < limit; it++) {
+        unsigned done = 0;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(smem_addr(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
 }  // namespace excent

@@ -24,6 +24,7 @@ static constexpr int SNAP_GROUP = 16;     // bitmap words per warp step in the s
 static constexpr unsigned HUB_MIN = 256;  // degree > 256: split into segments for whole warps
 static constexpr unsigned HUB_SEG = 1024; // edges per hub segment
 static constexpr int UNROLL = 4;          // independent index loads per lane in flight
+static constexpr int STAGE_INTS = 1024;   // per warp: shared-memory stage of a tile's short lists (4 KiB)
 static constexpr int BLOCK = 256;
 
 enum { SRC_TABLE = 0, SRC_CHUNK = 1, SRC_GATHER = 2, SRC_HOT = 3, SRC_HUBS = 4 };
@@ -132,6 +133,7 @@ struct PushArgs {
     const ull* hubv_cnt;
     int skip_hubs;      // SRC_TABLE leaves the lists longer than HUB_MIN to SRC_HUBS
     int chunk;          // SRC_TABLE: only chunk `chunk`'s items (-1: every chunk's)
+    int stage;          // SRC_CHUNK / SRC_GATHER: bulk-copy each tile's short lists into shared memory
     // lists past the device cache read in place from pinned host memory (zero copy)
     const int* hcache;   // entries [cache_edges, m), device-mapped
     ull cache_edges;
@@ -557,11 +559,21 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
     T* x = reinterpret_cast<T*>(a.x);
     T* r = reinterpret_cast<T*>(a.r);
     T* hacc = hacc_init<T>(a.hub_k);
+    // streamed and gathered lists: each tile's short lists arrive in shared memory by one bulk copy
+    constexpr bool STAGED = SRC == SRC_CHUNK || SRC == SRC_GATHER;
+    __shared__ __align__(16) int s_stage[STAGED ? BLOCK / 32 : 1][STAGED ? STAGE_INTS : 4];
+    __shared__ unsigned long long s_bar[BLOCK / 32];
     __shared__ const int* s_nb[BLOCK / 32][32];
     __shared__ unsigned s_ex[BLOCK / 32][32];
     __shared__ T s_p[BLOCK / 32][32];
     __shared__ ull s_pushed[3][BLOCK / 32];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    bool stage_on = STAGED && a.stage;
+    unsigned bar_phase = 0;
+    if (stage_on) {
+        if (lane == 0) bar_init(&s_bar[wib]);
+        __syncwarp();
+    }
     const long long first = item_first<SRC>(a), total = item_total<SRC>(a);
     const long long ntiles = total > first ? (total - first + 31) / 32 : 0;
     // claims of up to TILE_BATCH tiles, fewer when there are not two claims per warp
@@ -633,6 +645,30 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
             const int rank = __popc(nz & ((1u << lane) - 1u));
             if (ds) { s_nb[wib][rank] = nb; s_ex[wib][rank] = ex; s_p[wib][rank] = p; }
             __syncwarp();
+            // streamed / gathered tiles: consecutive items' lists lie back to back, so the
+            // short ones span one stretch; when it fits, one bulk copy brings it (16-byte
+            // aligned, the buffers are padded) and the entries are read from shared memory
+            const int* st_base = nullptr;
+            if (stage_on) {
+                unsigned long long lo = ds ? (unsigned long long)(uintptr_t)nb : ~0ull;
+                unsigned long long hi = ds ? (unsigned long long)(uintptr_t)(nb + ds) : 0ull;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    lo = min(lo, __shfl_xor_sync(FULL, lo, o));
+                    hi = max(hi, __shfl_xor_sync(FULL, hi, o));
+                }
+                const unsigned long long a0 = lo & ~15ull, a1 = (hi + 15ull) & ~15ull;
+                if (a1 - a0 <= (unsigned long long)STAGE_INTS * sizeof(int)) {
+                    if (lane == 0) bulk_stage(&s_bar[wib], s_stage[wib], (const void*)(uintptr_t)a0, (unsigned)(a1 - a0));
+                    const bool ok = __all_sync(FULL, bar_wait(&s_bar[wib], bar_phase, SPIN_LIMIT));
+                    bar_phase ^= 1u;
+                    if (ok) st_base = (const int*)(uintptr_t)a0;
+                    else {   // never expected: leave the stage alone from here on
+                        if (lane == 0) atomicExch(&a.ctrl->err, 3);
+                        stage_on = false;
+                    }
+                }
+            }
             const unsigned le = lane == 31 ? FULL : (2u << lane) - 1u;
             for (unsigned j0 = 0; j0 < tot; j0 += 32 * UNROLL) {
                 int u[UNROLL];
@@ -647,7 +683,12 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
                         __reduce_or_sync(FULL, (ds && ex >= wb && ex - wb < 32) ? 1u << (ex - wb) : 0u);
                     const int o = __popc(__ballot_sync(FULL, ds && ex <= wb)) - 1 + __popc(starts & le & ~1u);
                     own[k] = j < tot ? o : -1;
-                    u[k] = j < tot ? ld_edge(s_nb[wib][o] + (j - s_ex[wib][o])) : 0;
+                    if constexpr (STAGED) {
+                        if (st_base) u[k] = j < tot ? s_stage[wib][(s_nb[wib][o] - st_base) + (j - s_ex[wib][o])] : 0;
+                        else u[k] = j < tot ? ld_edge(s_nb[wib][o] + (j - s_ex[wib][o])) : 0;
+                    } else {
+                        u[k] = j < tot ? ld_edge(s_nb[wib][o] + (j - s_ex[wib][o])) : 0;
+                    }
                 }
 #pragma unroll
                 for (int k = 0; k < UNROLL; k++)
@@ -1080,7 +1121,8 @@ extern "C" int excent_engine_reserve_cache(excent_engine* e, unsigned long long 
     e->hub_k = 0;   // a fresh cache holds plain ids
     if (e->h_hcache) { cudaFreeHost(e->h_hcache); e->h_hcache = nullptr; e->hcache_edges = 0; }
     if (edges == 0) return EXCENT_OK;
-    if (cudaMalloc((void**)&e->d_cache, edges * sizeof(int)) != cudaSuccess) {
+    // 4 entries of padding: a bulk copy of a stretch rounds its end up to 16 bytes
+    if (cudaMalloc((void**)&e->d_cache, (edges + 4) * sizeof(int)) != cudaSuccess) {
         cudaGetLastError();
         e->d_cache = nullptr;
         EX_FAIL(EXCENT_ERR_NOMEM, "edge cache of %llu edges does not fit", edges);
@@ -1237,7 +1279,7 @@ static PushArgs push_args(excent_engine* e, int q) {
     a.hids = e->d_hids; a.hoff = e->d_hoff; a.hedges = e->d_hedges; a.hlist = e->d_hlist;
     a.hubq = e->d_hubq[q]; a.hub_cap = e->hub_cap[q]; a.q = e->d_queue + q; a.ctrl = e->d_ctrl;
     a.hub_id = e->d_hub_id; a.hub_k = e->hub_k;
-    a.hubv = e->d_hubv; a.hubv_cnt = e->d_hubv_cnt; a.skip_hubs = 0; a.chunk = -1;
+    a.hubv = e->d_hubv; a.hubv_cnt = e->d_hubv_cnt; a.skip_hubs = 0; a.chunk = -1; a.stage = 0;
     a.hcache = nullptr; a.cache_edges = e->cache_edges;
     if (e->h_hcache) cudaHostGetDevicePointer((void**)&a.hcache, e->h_hcache, 0);
     return a;
@@ -1306,7 +1348,7 @@ extern "C" int excent_engine_slots_create(excent_engine* e, unsigned long long m
     EX_CUDA(cudaSetDevice(e->dev));
     e->zc = zero_copy != 0;
     for (Slot& s : e->slot) {
-        const size_t eb = std::max<ull>(max_chunk_edges, 1) * sizeof(int);
+        const size_t eb = (std::max<ull>(max_chunk_edges, 1) + 4) * sizeof(int);   // + padding for bulk copies
         const size_t vb = (size_t)max_chunk_verts * sizeof(int), ob = ((size_t)max_chunk_verts + 1) * sizeof(ull);
         if (e->zc) {
             if (cudaHostAlloc((void**)&s.h_edges, eb, cudaHostAllocMapped) != cudaSuccess ||
@@ -1380,6 +1422,7 @@ extern "C" int excent_engine_push_stream(excent_engine* e, int s, int c, const u
     PushArgs a = push_args(e, 1 + s);
     a.hot = e->hot_skip ? e->d_hot : nullptr;
     a.cv_0 = v0; a.ebase = dst; a.e0 = e0;
+    a.stage = e->zc ? 0 : 1;   // mapped host slots are read in place
     if ((double)k < list_frac * nv) { a.ctype = WT_LIST; a.ccount = (unsigned)k; e->n_list++; }
     else { a.ctype = WT_RANGE; a.ccount = (unsigned)nv; e->n_range++; }
     if (a.ccount) launch_push<SRC_CHUNK>(e, a, grid_for(e, a.ccount), sl.st);
@@ -1403,6 +1446,7 @@ extern "C" int excent_engine_push_gather(excent_engine* e, int s, int k, unsigne
     if (k) {
         PushArgs a = push_args(e, 1 + s);
         a.vids = sl.d_vids; a.off = sl.d_off; a.gedges = sl.d_edges; a.gk = (unsigned)k;
+        a.stage = e->zc ? 0 : 1;
         launch_push<SRC_GATHER>(e, a, grid_for(e, (ull)k), sl.st);
         EX_CUDA(cudaGetLastError());
     }
