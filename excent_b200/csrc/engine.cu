@@ -504,6 +504,57 @@ __device__ __forceinline__ long long item_total(const PushArgs& a) {
 // index below the tail has been reserved by a warp that writes it without
 // waiting on anything, so the wait for its tag ends; the waits are still
 // bounded (about a second), after which ctrl->err = 2 and the warp stops.
+// Scatter queued segment i (reserved, so its tag is set soon): wait for the tag
+// (bounded), read it, clear the tag for the next launch, scatter. False if the
+// wait gave up (ctrl->err = 2).
+template <typename T>
+__device__ __forceinline__ bool scatter_segment(const PushArgs& a, T* r, T* hacc, int lane, ull i) {
+    int ok = 1;
+    if (lane == 0) {
+        unsigned it = 0;
+        while (!*(volatile unsigned*)&a.hubq[i].tag) {
+            if (++it >= SPIN_LIMIT) { atomicExch(&a.ctrl->err, 2); ok = 0; break; }
+            __nanosleep(64);
+        }
+    }
+    if (!__shfl_sync(FULL, ok, 0)) return false;
+    __threadfence();
+    const HubSeg* hs = a.hubq + i;
+    const int* nb = (const int*)__ldcg((const unsigned long long*)&hs->nb);
+    const unsigned len = __ldcg(&hs->len);
+    const float4 p4 = __ldcg(&hs->p);
+    __syncwarp();
+    if (lane == 0) *(volatile unsigned*)&a.hubq[i].tag = 0u;   // the slot is clean for the next launch
+    T p;
+    if constexpr (sizeof(T) == sizeof(float)) p = p4.x; else p = p4;
+    warp_scatter(r, nb, len, p, lane, hacc);
+    return true;
+}
+
+// Between batches of tiles: scatter the segments queued so far (claimed only
+// while the head is below the tail), so a long list's residual spreads soon
+// after it was taken, as a vertex's own scatter follows its take.
+template <typename T>
+__device__ __forceinline__ void help_segments(const PushArgs& a, T* r, T* hacc, int lane) {
+    for (;;) {
+        ull i = 0;
+        int got = 0;
+        if (lane == 0) {
+            ull h = *(volatile ull*)&a.q->head;
+            const ull t = *(volatile ull*)&a.q->tail;
+            while (h < t) {
+                const ull prev = atomicCAS(&a.q->head, h, h + 1);
+                if (prev == h) { got = 1; i = h; break; }
+                h = prev;
+            }
+        }
+        if (!__shfl_sync(FULL, got, 0)) return;
+        i = __shfl_sync(FULL, i, 0);
+        if (i >= a.hub_cap) continue;   // never written (the producer flagged the overflow)
+        if (!scatter_segment(a, r, hacc, lane, i)) return;
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ void drain_segments(const PushArgs& a, T* r, T* hacc, int lane, long long nbatch) {
     for (;;) {
@@ -513,9 +564,9 @@ __device__ __forceinline__ void drain_segments(const PushArgs& a, T* r, T* hacc,
             i = atomicAdd(&a.q->head, 1ull);
             for (unsigned it = 0;; it++) {
                 const ull tail = *(volatile ull*)&a.q->tail;
-                if (i < tail) {
-                    if (i >= a.hub_cap) { state = 3; break; }   // never written (the producer flagged it)
-                    if (*(volatile unsigned*)&a.hubq[i].tag) { state = 1; break; }
+                if (i < tail) {   // reserved: it is (or soon will be) written
+                    state = i >= a.hub_cap ? 3 : 1;   // past the capacity: never written (the producer flagged it)
+                    break;
                 } else {
                     const ull cw = *(volatile ull*)&a.q->claim;
                     if ((long long)(cw >> 32) >= nbatch && (cw & 0xffffffffull) == 0) {
@@ -532,16 +583,7 @@ __device__ __forceinline__ void drain_segments(const PushArgs& a, T* r, T* hacc,
         if (state == 2) return;
         if (state == 3) continue;
         i = __shfl_sync(FULL, i, 0);
-        __threadfence();
-        const HubSeg* hs = a.hubq + i;
-        const int* nb = (const int*)__ldcg((const unsigned long long*)&hs->nb);
-        const unsigned len = __ldcg(&hs->len);
-        const float4 p4 = __ldcg(&hs->p);
-        __syncwarp();
-        if (lane == 0) *(volatile unsigned*)&a.hubq[i].tag = 0u;   // the slot is clean for the next launch
-        T p;
-        if constexpr (sizeof(T) == sizeof(float)) p = p4.x; else p = p4;
-        warp_scatter(r, nb, len, p, lane, hacc);
+        if (!scatter_segment(a, r, hacc, lane, i)) return;
     }
 }
 
@@ -702,6 +744,7 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
     __threadfence();
     if (lane == 0) atomicAdd(&a.q->claim, ~0ull);
     if (batch >= nbatch) break;
+    help_segments<T>(a, r, hacc, lane);
     }
     // out of tiles: scatter queued long-list segments until none is left or coming
     drain_segments<T>(a, r, hacc, lane, nbatch);
@@ -1941,7 +1984,7 @@ extern "C" int excent_engine_set_hub_targets(excent_engine* e, int k) {
         EX_CUDA(cudaGetLastError());
     }
     const size_t smem = hub_smem(e);
-    if (smem > 48 * 1024) {   // above the default dynamic shared memory limit: opt in, per kernel
+    if (smem > 0) {   // static + dynamic above 48 KiB needs the opt-in, per kernel (the staged kernels hold ~40 KiB)
         const int sz = (int)smem;
         cudaFuncSetAttribute(k_push<1, SRC_TABLE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz);
         cudaFuncSetAttribute(k_push<1, SRC_CHUNK>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz);
