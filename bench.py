@@ -95,8 +95,11 @@ def parse():
     ap.add_argument("--list-frac", type=float, default=0.5,
                     help="per-chunk list/range rule of the device loop (the reference's --list-frac)")
     ap.add_argument("--log-dir", default=None, help="keep the stdout of every CLI run in this directory")
-    ap.add_argument("--hub-order", default="first", choices=["first", "last", "table"],
-                    help="where the high-degree lists go in each pass of the device loop")
+    ap.add_argument("--hub-order", default="auto", choices=["auto", "first", "last", "table"],
+                    help="where the high-degree lists go in each pass of the device loop (auto: table order when "
+                         "the chunks are swept one by one, else first)")
+    ap.add_argument("--chunk-sweep", default="auto", choices=["auto", "on", "off"],
+                    help="cached pushes one chunk per launch in chunk order (auto: when there are several chunks)")
     ap.add_argument("--hub-targets", type=int, default=-1,
                     help="shared-memory aggregation of the k highest-degree targets (0: off; -1: 16384 for "
                          "one measure, 4096 for all)")
@@ -240,6 +243,7 @@ def error_report(a, n, m, d_idx, d_adj, idx_np, adj_np, v0, e, eng, meas, measur
         eng2.upload_device(d_idx, d_adj)
         eng2.set_hub_targets(min(4096, n))
         eng2.set_hub_order(a.hub_order)
+        eng2.set_chunk_sweep({"auto": "auto", "on": True, "off": False}[a.chunk_sweep])
         st = eng2.solve(list_frac=a.list_frac, max_passes=a.ref_passes)
         rep["like_for_like"] = {"ev_init": "lambda1 rounded to float", "ev_project": "off",
                                 "max_passes": a.ref_passes, "passes": st.passes,
@@ -311,6 +315,7 @@ def run_ours(a, world, rank, local, dist):
     hub_k = a.hub_targets if a.hub_targets >= 0 else min(16384 if nm == 1 else 4096, n)
     eng.set_hub_targets(hub_k)
     eng.set_hub_order(a.hub_order)
+    eng.set_chunk_sweep({"auto": "auto", "on": True, "off": False}[a.chunk_sweep])
     use_graph = not a.no_graph
     for _ in range(a.warmup):
         s = eng.solve(list_frac=a.list_frac, use_graph=use_graph)
@@ -405,7 +410,7 @@ def run_ours(a, world, rank, local, dist):
                    "cuda_graph": use_graph, "parallelism": f"{world} independent replicas",
                    "ev_init": a.ev_init, "ev_project": a.ev_project if measure == "all" else None,
                    "hub_targets": hub_k, "list_frac": a.list_frac,
-                   "hub_order": a.hub_order},
+                   "hub_order": a.hub_order, "chunk_sweep": a.chunk_sweep},
         "e2e": {"value": round(e_pushed / te / 1e9, 4), "unit": "GTEPS", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": round(te / a.steps * 1e3, 3),
                 "wall_ms_per_step": round(te_wall / a.steps * 1e3, 3)},

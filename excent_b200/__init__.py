@@ -209,7 +209,7 @@ class Engine:
     def set_hub_order(self, order="first"):
         """Device solve: where the lists longer than 256 entries go in each pass
         ("first", "last", or "table": with the rest)."""
-        code = {"table": 0, "first": 1, "last": 2, False: 0, True: 1}[order]
+        code = {"auto": -1, "table": 0, "first": 1, "last": 2, False: 0, True: 1}[order]
         call("excent_engine_set_hub_order", self.h, code)
 
     def autotune(self, list_frac=0.5, max_passes=100000):
@@ -231,8 +231,9 @@ class Engine:
         return v.value
 
     def set_chunk_sweep(self, on=True):
-        """Cached pushes one chunk per launch, in chunk order (the reference's launch order)."""
-        call("excent_engine_set_chunk_sweep", self.h, int(bool(on)))
+        """Cached pushes one chunk per launch, in chunk order (the reference's launch order);
+        "auto": when the graph has more than one chunk."""
+        call("excent_engine_set_chunk_sweep", self.h, -1 if on == "auto" else int(bool(on)))
 
     def host_cache(self):
         """Pinned host memory for the entries past the edge cache (excent_engine_host_cache):

@@ -912,8 +912,8 @@ struct excent_engine {
     int* d_hubv = nullptr;   // high-degree-first order: vertices with lists longer than HUB_MIN
     ull* d_hubv_cnt = nullptr;
     ull hubv_cap = 0;
-    int hub_order = 1;       // high-degree lists: 0 in table order, 1 first, 2 last
-    bool chunk_sweep = false; // cached pushes chunk by chunk, each launch after the previous one
+    int hub_order = -1;      // high-degree lists: 0 in table order, 1 first, 2 last, -1 by the chunk count
+    int sweep_mode = -1;     // cached pushes chunk by chunk (1), in one launch (0), -1 by the chunk count
     cudaGraphConditionalHandle* d_chunk_if = nullptr;  // per chunk: does this pass push it (graph IF nodes)
     std::vector<cudaGraphConditionalHandle> h_chunk_if;
     bool hubv_stale = true;
@@ -961,6 +961,19 @@ static void invalidate_graph(excent_engine* e) {
 }
 
 static void scrub_queues(excent_engine* e);
+static int ensure_hubv(excent_engine* e);
+
+// Pass order. By default a graph cut into several chunks is pushed chunk by
+// chunk, each chunk's long lists in their place, which is how the reference
+// launches its resident chunks (src/excent.cu:684-688): every chunk then sees
+// what the earlier ones pushed in the same pass, and a solve pushes about as
+// many entries as the reference's. A single chunk pushes its high-degree
+// lists first instead (measured: fewer entries and smaller errors than table
+// order there). Both can be set explicitly.
+static bool sweep_of(const excent_engine* e) { return e->sweep_mode >= 0 ? e->sweep_mode != 0 : e->nc > 1; }
+static int order_of(const excent_engine* e) { return e->hub_order >= 0 ? e->hub_order : (sweep_of(e) ? 0 : 1); }
+// the order a pass can run: a high-degree order needs the listed high-degree vertices
+static int effective_order(const excent_engine* e);
 
 static int free_engine(excent_engine* e) {
     if (!e) return EXCENT_OK;
@@ -1370,7 +1383,17 @@ extern "C" int excent_engine_push_cached(excent_engine* e, const unsigned char* 
                             cudaMemcpyHostToDevice, e->s_main));
     PushArgs a = push_args(e, 0);
     a.hot = e->hot_skip ? e->d_hot : nullptr;
-    if (e->chunk_sweep) {   // one launch (and its hub segments) per chunk, in chunk order
+    // a high-degree order needs every chunk with work in the cache (the hub list spans the graph)
+    bool all_cached = true;
+    for (int c = 0; c < e->nc; c++) all_cached &= cnt[2 * c] == 0 || mode[c] == 1;
+    int order = 0;
+    if (all_cached && order_of(e) && !sweep_of(e)) {
+        EX_TRY(ensure_hubv(e));
+        order = effective_order(e);
+    }
+    if (order == 1) launch_push<SRC_HUBS>(e, a, e->grid_push, e->s_main);
+    a.skip_hubs = order != 0;
+    if (sweep_of(e)) {   // one launch per chunk, in chunk order
         for (int c = 0; c < e->nc; c++) {
             const unsigned items = e->h_wt_prefix[c + 1] - e->h_wt_prefix[c];
             if (!items) continue;
@@ -1380,6 +1403,8 @@ extern "C" int excent_engine_push_cached(excent_engine* e, const unsigned char* 
     } else {
         launch_push<SRC_TABLE>(e, a, grid_for(e, total), e->s_main);
     }
+    a.skip_hubs = 0;
+    if (order == 2) launch_push<SRC_HUBS>(e, a, e->grid_push, e->s_main);
     EX_CUDA(cudaGetLastError());
     return EXCENT_OK;
 }
@@ -1620,13 +1645,10 @@ static cudaError_t close_if(cudaStream_t body) {
 // Kernels of one pass outside the per-chunk launches of a chunk sweep, and per
 // chunk launch (for the launch count of a graph solve).
 static void pass_kernels(const excent_engine* e, int order, ull* fixed, ull* per_chunk) {
-    *fixed = 2 + (order == 1 || order == 2 ? 1 : 0) + (e->chunk_sweep ? 0 : 1);
-    *per_chunk = e->chunk_sweep ? 1 : 0;
+    *fixed = 2 + (order == 1 || order == 2 ? 1 : 0) + (sweep_of(e) ? 0 : 1);
+    *per_chunk = sweep_of(e) ? 1 : 0;
 }
 
-static int effective_order(const excent_engine* e) {
-    return e->hub_order && e->d_hubv && !e->hubv_stale ? e->hub_order : 0;
-}
 
 // One pass of the device solve: snapshot -> plan -> push -> hub segments.
 // With ev, events are recorded between the kernels. chunk_body (a second
@@ -1639,7 +1661,7 @@ static cudaError_t enqueue_pass(excent_engine* e, double list_frac, int max_pass
     if (ev) cudaEventRecord(ev[0], st);
     launch_snapshot(e, false, st);
     if (ev) cudaEventRecord(ev[1], st);
-    const bool use_if = chunk_body && e->chunk_sweep;
+    const bool use_if = chunk_body && sweep_of(e);
     k_plan<<<1, 1024, 0, st>>>(e->nc, e->d_cv0, e->n, e->d_cnt, e->d_cmode, list_frac, max_passes, e->d_wt_type,
                                e->d_wt_prefix, e->d_ctrl, e->d_queue, e->d_log, e->log_cap, cond, use_cond,
                                use_if ? e->d_chunk_if : nullptr);
@@ -1664,7 +1686,7 @@ static cudaError_t enqueue_pass(excent_engine* e, double list_frac, int max_pass
     };
     if (order == 1) hub_phase();
     a.skip_hubs = order != 0;   // the table push skips the high-degree vertices
-    if (e->chunk_sweep) {
+    if (sweep_of(e)) {
         // chunk by chunk: each chunk's push (with its long lists) completes before the next
         // chunk's vertices are taken, so they see everything pushed so far
         for (int c = 0; c < e->nc; c++) {
@@ -1695,7 +1717,7 @@ static cudaError_t enqueue_pass(excent_engine* e, double list_frac, int max_pass
 static int build_graph(excent_engine* e, double list_frac, int max_passes) {
     if (e->gexec && e->graph_max_passes == max_passes && e->graph_list_frac == list_frac) return EXCENT_OK;
     invalidate_graph(e);
-    if (e->chunk_sweep && !e->d_chunk_if) EX_ALLOC(e->d_chunk_if, (size_t)e->nc * sizeof(cudaGraphConditionalHandle));
+    if (sweep_of(e) && !e->d_chunk_if) EX_ALLOC(e->d_chunk_if, (size_t)e->nc * sizeof(cudaGraphConditionalHandle));
     e->h_chunk_if.assign(e->nc, 0);
     cudaGraph_t g;
     EX_CUDA(cudaGraphCreate(&g, 0));
@@ -1715,7 +1737,7 @@ static int build_graph(excent_engine* e, double list_frac, int max_passes) {
     EX_CUDA(cudaStreamCreateWithFlags(&cb, cudaStreamNonBlocking));
     EX_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     const ull before = e->launches;
-    const cudaError_t pe = enqueue_pass(e, list_frac, max_passes, h, 1, cs, nullptr, e->chunk_sweep ? cb : nullptr);
+    const cudaError_t pe = enqueue_pass(e, list_frac, max_passes, h, 1, cs, nullptr, sweep_of(e) ? cb : nullptr);
     e->launches = before;
     cudaGraph_t captured;
     const cudaError_t ce = cudaStreamEndCapture(cs, &captured);
@@ -1726,7 +1748,7 @@ static int build_graph(excent_engine* e, double list_frac, int max_passes) {
         cudaGetLastError();
         EX_CUDA(pe != cudaSuccess ? pe : ce);
     }
-    if (e->chunk_sweep)
+    if (sweep_of(e))
         EX_CUDA(cudaMemcpy(e->d_chunk_if, e->h_chunk_if.data(), (size_t)e->nc * sizeof(cudaGraphConditionalHandle),
                            cudaMemcpyHostToDevice));
     const cudaError_t ie = cudaGraphInstantiate(&e->gexec, g, 0);
@@ -1784,20 +1806,14 @@ extern "C" int excent_engine_seed(excent_engine* e, int k, const int32_t* vids, 
     return EXCENT_OK;
 }
 
-static int solve_impl(excent_engine* e, double list_frac, int max_passes, int use_graph, bool init) {
-    EX_CHECK_ARG(e, "null engine");
-    EX_CHECK_ARG(max_passes >= 0 && max_passes < e->log_cap, "max_passes must be < %d", e->log_cap);
-    for (int c = 0; c < e->nc; c++)
-        EX_CHECK_ARG(e->loaded[c] || (e->h_hcache && e->ce[c] >= e->cache_edges),
-                     "chunk %d is neither in the edge cache nor in the host cache", c);
-    EX_CUDA(cudaSetDevice(e->dev));
-    std::vector<uint8_t> cm(e->nc, 1);
-    for (int c = 0; c < e->nc; c++)
-        if (e->h_hcache && e->ce[c] >= e->cache_edges) cm[c] = 2;   // lists in host memory
-    EX_CUDA(cudaMemcpy(e->d_cmode, cm.data(), e->nc, cudaMemcpyHostToDevice));
-    if (init) EX_TRY(init_state(e));
-    else EX_TRY(reset_counters(e));
-    if (e->hub_order && e->hubv_stale) {
+// The vertices whose lists are longer than HUB_MIN (for a high-degree order),
+// listed once per graph; without room for the list the solve runs in table order.
+static int effective_order(const excent_engine* e) {
+    return order_of(e) && e->d_hubv && !e->hubv_stale ? order_of(e) : 0;
+}
+
+static int ensure_hubv(excent_engine* e) {
+    if (e->hubv_stale) {
         // count the high-degree vertices, then list them in a buffer of that size
         if (!e->d_hubv_cnt) EX_ALLOC(e->d_hubv_cnt, sizeof(ull));
         EX_CUDA(cudaMemsetAsync(e->d_hubv_cnt, 0, sizeof(ull), e->s_main));
@@ -1825,6 +1841,23 @@ static int solve_impl(excent_engine* e, double list_frac, int max_passes, int us
             e->hubv_stale = false;
         }
     }
+    return EXCENT_OK;
+}
+
+static int solve_impl(excent_engine* e, double list_frac, int max_passes, int use_graph, bool init) {
+    EX_CHECK_ARG(e, "null engine");
+    EX_CHECK_ARG(max_passes >= 0 && max_passes < e->log_cap, "max_passes must be < %d", e->log_cap);
+    for (int c = 0; c < e->nc; c++)
+        EX_CHECK_ARG(e->loaded[c] || (e->h_hcache && e->ce[c] >= e->cache_edges),
+                     "chunk %d is neither in the edge cache nor in the host cache", c);
+    EX_CUDA(cudaSetDevice(e->dev));
+    std::vector<uint8_t> cm(e->nc, 1);
+    for (int c = 0; c < e->nc; c++)
+        if (e->h_hcache && e->ce[c] >= e->cache_edges) cm[c] = 2;   // lists in host memory
+    EX_CUDA(cudaMemcpy(e->d_cmode, cm.data(), e->nc, cudaMemcpyHostToDevice));
+    if (init) EX_TRY(init_state(e));
+    else EX_TRY(reset_counters(e));
+    if (order_of(e)) EX_TRY(ensure_hubv(e));
     if (use_graph) {
         EX_TRY(build_graph(e, list_frac, max_passes));
         EX_CUDA(cudaGraphLaunch(e->gexec, e->s_main));
@@ -2006,7 +2039,8 @@ extern "C" int excent_engine_set_hub_targets(excent_engine* e, int k) {
 }
 
 extern "C" int excent_engine_set_hub_order(excent_engine* e, int order) {
-    EX_CHECK_ARG(e && order >= 0 && order <= 2, "hub order must be 0 (table order), 1 (first) or 2 (last)");
+    EX_CHECK_ARG(e && order >= -1 && order <= 2,
+                 "hub order must be 0 (table order), 1 (first), 2 (last) or -1 (by the chunk count)");
     EX_CUDA(cudaSetDevice(e->dev));
     invalidate_graph(e);
     e->hub_order = order;
@@ -2114,7 +2148,7 @@ extern "C" int excent_engine_set_chunk_sweep(excent_engine* e, int on) {
     EX_CHECK_ARG(e, "null engine");
     EX_CUDA(cudaSetDevice(e->dev));
     invalidate_graph(e);
-    e->chunk_sweep = on != 0;
+    e->sweep_mode = on < 0 ? -1 : (on != 0);
     return EXCENT_OK;
 }
 

@@ -50,9 +50,9 @@ struct Options {
     bool device_loop = false;  // fully cached graphs: load at setup, run the on-device pass loop
     bool ev_init_fp64 = false; // eigenvector initial residual from the FP64 lambda1
     int hub_targets = -1;      // shared-memory aggregation of the top-degree targets (-1: auto)
-    int hub_order = 1;         // device loop: the high-degree lists 0 in table order, 1 first, 2 last
+    int hub_order = -1;        // the high-degree lists 0 in table order, 1 first, 2 last, -1 by the chunk count
     std::string host_cache = "off";   // pinned: entries past the HBM cache read in place from pinned host memory
-    bool chunk_sweep = false;  // cached pushes one chunk per launch, in chunk order
+    int chunk_sweep = -1;      // cached pushes one chunk per launch (1), in one launch (0), -1 by the chunk count
 };
 
 static const char* USAGE =
@@ -125,8 +125,11 @@ static int parse_options(int argc, char** argv, Options& o) {
         }
         else if (a == "--chunk-sweep") {
             if ((ok = next(v))) {
-                if (strcmp(v, "on") && strcmp(v, "off")) { fprintf(stderr, "--chunk-sweep must be on or off\n"); return 1; }
-                o.chunk_sweep = !strcmp(v, "on");
+                if (strcmp(v, "on") && strcmp(v, "off") && strcmp(v, "auto")) {
+                    fprintf(stderr, "--chunk-sweep must be on, off or auto\n");
+                    return 1;
+                }
+                o.chunk_sweep = !strcmp(v, "auto") ? -1 : !strcmp(v, "on");
             }
         }
         else if (a == "--hub-order") {
@@ -134,7 +137,8 @@ static int parse_options(int argc, char** argv, Options& o) {
                 if (!strcmp(v, "table")) o.hub_order = 0;
                 else if (!strcmp(v, "first")) o.hub_order = 1;
                 else if (!strcmp(v, "last")) o.hub_order = 2;
-                else { fprintf(stderr, "--hub-order must be first, last or table\n"); return 1; }
+                else if (!strcmp(v, "auto")) o.hub_order = -1;
+                else { fprintf(stderr, "--hub-order must be first, last, table or auto\n"); return 1; }
             }
         }
         else { fprintf(stderr, "unknown option %s\n", a.c_str()); return 1; }
@@ -466,7 +470,7 @@ private:
             }
         }
         RT_CK(excent_engine_set_hub_order(e_, o_.hub_order));
-        RT_CK(excent_engine_set_chunk_sweep(e_, o_.chunk_sweep ? 1 : 0));
+        RT_CK(excent_engine_set_chunk_sweep(e_, o_.chunk_sweep));
         hot_mode_ = cache_mode_ == "hot";
         if (hot_mode_) return setup_degree_cache(reserve);
         return 0;

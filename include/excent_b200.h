@@ -237,15 +237,16 @@ int excent_engine_read_trace(excent_engine* e, uint16_t* out);
 int excent_engine_set_hub_targets(excent_engine* e, int k);
 
 /* Order of the high-degree lists (more than 256 entries) in each pass of the
- * device solve: 1 (default) first, so the large share of a pass's residual they
- * carry reaches the other vertices before those are taken; 2 last, after every
- * other pending vertex, so they collect the pass's residual and push it once;
- * 0 in table order with the rest. No reference counterpart (the reference
- * pushes chunk by chunk, its degree cache at the end of a pass by default). */
+ * device solve and of a host-driven cached push: 1 first, so the large share
+ * of a pass's residual they carry reaches the other vertices before those are
+ * taken; 2 last, after every other pending vertex; 0 in table order with the
+ * rest; -1 (the default) table order when the chunks are swept one by one,
+ * else first. */
 int excent_engine_set_hub_order(excent_engine* e, int order);
-/* Cached pushes chunk by chunk (on: one launch per chunk, each after the
+/* Cached pushes chunk by chunk (1: one launch per chunk, each after the
  * previous one, as the reference launches its resident chunks on one stream,
- * src/excent.cu:684-688), or every chunk in one launch (off, the default). */
+ * src/excent.cu:684-688), every chunk in one launch (0), or -1 (the default):
+ * chunk by chunk when the graph has more than one chunk. */
 int excent_engine_set_chunk_sweep(excent_engine* e, int on);
 /* The scatter's ceiling on this graph: one reduction per edge-cache entry (in
  * cache order, to its target, into a scratch array shaped like the residuals),
