@@ -38,14 +38,15 @@ struct HubSeg {
 };
 
 // The work queue of one push launch: tiles are claimed in batches from
-// `claim` (high 32 bits: batches claimed, low 32 bits: warps still working on
-// a batch), long lists are queued as segments at `tail` and taken from `head`
-// by warps that ran out of tiles. Zeroed before every launch.
+// `claim` (high 32 bits: batches claimed), long lists are queued as segments
+// at `tail` and taken from `head` by warps between batches; k_segments takes
+// the rest after the launch. Zeroed before every launch.
 struct PushQueue {
     ull tail, head, claim, pad;
 };
-static constexpr int TILE_BATCH = 8;            // at most this many tiles (of 32 items) per claim
-static constexpr unsigned SPIN_LIMIT = 1u << 24; // bounded waits for a queued segment (about a second)
+static constexpr int TILE_BATCH = 32;           // at most this many tiles (of 32 items) per claim
+static constexpr unsigned SPIN_LIMIT = 1u << 24; // bounded polls of an mbarrier
+static constexpr long long WAIT_CYCLES = 2000000000ll;   // bounded wait for a reserved segment's tag (about a second)
 
 // Device control block: counters that live across kernels of one pass.
 struct Ctrl {
@@ -498,12 +499,6 @@ __device__ __forceinline__ long long item_total(const PushArgs& a) {
     else return a.ctrl->hcount;
 }
 
-// A warp that ran out of tiles takes queued segments of long lists (HUB_SEG
-// entries each) one at a time and scatters them, until every batch of tiles
-// has been claimed and finished and the queue is empty. A claimed segment
-// index below the tail has been reserved by a warp that writes it without
-// waiting on anything, so the wait for its tag ends; the waits are still
-// bounded (about a second), after which ctrl->err = 2 and the warp stops.
 // Scatter queued segment i (reserved, so its tag is set soon): wait for the tag
 // (bounded), read it, clear the tag for the next launch, scatter. False if the
 // wait gave up (ctrl->err = 2).
@@ -511,9 +506,9 @@ template <typename T>
 __device__ __forceinline__ bool scatter_segment(const PushArgs& a, T* r, T* hacc, int lane, ull i) {
     int ok = 1;
     if (lane == 0) {
-        unsigned it = 0;
+        const long long t0 = clock64();
         while (!*(volatile unsigned*)&a.hubq[i].tag) {
-            if (++it >= SPIN_LIMIT) { atomicExch(&a.ctrl->err, 2); ok = 0; break; }
+            if (clock64() - t0 > WAIT_CYCLES) { atomicExch(&a.ctrl->err, 2); ok = 0; break; }
             __nanosleep(64);
         }
     }
@@ -555,36 +550,19 @@ __device__ __forceinline__ void help_segments(const PushArgs& a, T* r, T* hacc, 
     }
 }
 
-template <typename T>
-__device__ __forceinline__ void drain_segments(const PushArgs& a, T* r, T* hacc, int lane, long long nbatch) {
-    for (;;) {
-        ull i = 0;
-        int state = 0;   // 1 the segment is ready, 2 nothing more to do, 3 an index past the queue's capacity
-        if (lane == 0) {
-            i = atomicAdd(&a.q->head, 1ull);
-            for (unsigned it = 0;; it++) {
-                const ull tail = *(volatile ull*)&a.q->tail;
-                if (i < tail) {   // reserved: it is (or soon will be) written
-                    state = i >= a.hub_cap ? 3 : 1;   // past the capacity: never written (the producer flagged it)
-                    break;
-                } else {
-                    const ull cw = *(volatile ull*)&a.q->claim;
-                    if ((long long)(cw >> 32) >= nbatch && (cw & 0xffffffffull) == 0) {
-                        __threadfence();
-                        if (i >= *(volatile ull*)&a.q->tail) { state = 2; break; }
-                        continue;   // reserved meanwhile: wait for its tag
-                    }
-                }
-                if (it >= SPIN_LIMIT) { atomicExch(&a.ctrl->err, 2); state = 2; break; }
-                __nanosleep(100);
-            }
-        }
-        state = __shfl_sync(FULL, state, 0);
-        if (state == 2) return;
-        if (state == 3) continue;
-        i = __shfl_sync(FULL, i, 0);
-        if (!scatter_segment(a, r, hacc, lane, i)) return;
-    }
+// Segments still queued when a push launch ends (reserved after the last
+// help, or never helped): one warp per segment, right after the launch.
+template <int L>
+__global__ void __launch_bounds__(BLOCK) k_segments(void* rv, PushArgs a) {
+    typedef typename Lane<L>::T T;
+    T* r = reinterpret_cast<T*>(rv);
+    T* hacc = hacc_init<T>(a.hub_k);
+    const int lane = threadIdx.x & 31;
+    const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const ull head = a.q->head, tail = min(a.q->tail, a.hub_cap);
+    for (ull i = head + gw; i < tail; i += nwarps) scatter_segment(a, r, hacc, lane, i);
+    hacc_flush(hacc, r, a.hub_id, a.hub_k);
 }
 
 // Push kernel (persistent grid, warp tiles of 32 items). Each lane takes one
@@ -618,15 +596,15 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
     }
     const long long first = item_first<SRC>(a), total = item_total<SRC>(a);
     const long long ntiles = total > first ? (total - first + 31) / 32 : 0;
-    // claims of up to TILE_BATCH tiles, fewer when there are not two claims per warp
+    // claims of up to TILE_BATCH tiles, fewer when there are not four claims per warp
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    const long long per_claim = max(1ll, min((long long)TILE_BATCH, ntiles / (2 * nwarps)));
+    const long long per_claim = max(1ll, min((long long)TILE_BATCH, ntiles / (4 * nwarps)));
     const long long nbatch = (ntiles + per_claim - 1) / per_claim;
     ull pushed = 0, hpushed = 0, lanes = 0, taken = 0;
     for (;;) {
     // claim the next batch of tiles (and count this warp as working on it)
     ull claim = 0;
-    if (lane == 0) claim = atomicAdd(&a.q->claim, (1ull << 32) | 1ull);
+    if (lane == 0) claim = atomicAdd(&a.q->claim, 1ull << 32);
     const long long batch = (long long)(__shfl_sync(FULL, claim, 0) >> 32);
     const long long tile_end = batch < nbatch ? min((batch + 1) * per_claim, ntiles) : 0;
     for (long long tile = batch * per_claim; tile < tile_end; tile++) {
@@ -739,15 +717,11 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
             __syncwarp();
         }
     }
-    // done with the batch: its segments are reserved (and written) before the release
     __syncwarp();
-    __threadfence();
-    if (lane == 0) atomicAdd(&a.q->claim, ~0ull);
-    if (batch >= nbatch) break;
+    // between batches, and once more when out of tiles: the segments queued so far
     help_segments<T>(a, r, hacc, lane);
+    if (batch >= nbatch) break;
     }
-    // out of tiles: scatter queued long-list segments until none is left or coming
-    drain_segments<T>(a, r, hacc, lane, nbatch);
     pushed = warp_sum(pushed);
     lanes = warp_sum(lanes);
     taken = warp_sum(taken);
@@ -1346,9 +1320,14 @@ static PushArgs push_args(excent_engine* e, int q) {
 template <int SRC>
 static void launch_push(excent_engine* e, const PushArgs& a, int grid, cudaStream_t st) {
     cudaMemsetAsync(a.q, 0, sizeof(PushQueue), st);
-    if (e->L == 1) k_push<1, SRC><<<grid, BLOCK, hub_smem(e), st>>>(a);
-    else k_push<4, SRC><<<grid, BLOCK, hub_smem(e), st>>>(a);
-    e->launches++;
+    if (e->L == 1) {
+        k_push<1, SRC><<<grid, BLOCK, hub_smem(e), st>>>(a);
+        k_segments<1><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a);
+    } else {
+        k_push<4, SRC><<<grid, BLOCK, hub_smem(e), st>>>(a);
+        k_segments<4><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a);
+    }
+    e->launches += 2;
 }
 
 static int grid_for(excent_engine* e, ull items) {
@@ -1645,8 +1624,8 @@ static cudaError_t close_if(cudaStream_t body) {
 // Kernels of one pass outside the per-chunk launches of a chunk sweep, and per
 // chunk launch (for the launch count of a graph solve).
 static void pass_kernels(const excent_engine* e, int order, ull* fixed, ull* per_chunk) {
-    *fixed = 2 + (order == 1 || order == 2 ? 1 : 0) + (sweep_of(e) ? 0 : 1);
-    *per_chunk = sweep_of(e) ? 1 : 0;
+    *fixed = 2 + (order == 1 || order == 2 ? 2 : 0) + (sweep_of(e) ? 0 : 2);
+    *per_chunk = sweep_of(e) ? 2 : 0;
 }
 
 
@@ -1674,15 +1653,25 @@ static cudaError_t enqueue_pass(excent_engine* e, double list_frac, int max_pass
     const int order = effective_order(e);
     auto table = [&](cudaStream_t s) {
         cudaMemsetAsync(a.q, 0, sizeof(PushQueue), s);
-        if (e->L == 1) k_push<1, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), s>>>(a);
-        else k_push<4, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), s>>>(a);
-        e->launches++;
+        if (e->L == 1) {
+            k_push<1, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), s>>>(a);
+            k_segments<1><<<e->grid_push, BLOCK, hub_smem(e), s>>>(e->d_r, a);
+        } else {
+            k_push<4, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), s>>>(a);
+            k_segments<4><<<e->grid_push, BLOCK, hub_smem(e), s>>>(e->d_r, a);
+        }
+        e->launches += 2;
     };
     auto hub_phase = [&]() {
         cudaMemsetAsync(a.q, 0, sizeof(PushQueue), st);
-        if (e->L == 1) k_push<1, SRC_HUBS><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
-        else k_push<4, SRC_HUBS><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
-        e->launches++;
+        if (e->L == 1) {
+            k_push<1, SRC_HUBS><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
+            k_segments<1><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a);
+        } else {
+            k_push<4, SRC_HUBS><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
+            k_segments<4><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a);
+        }
+        e->launches += 2;
     };
     if (order == 1) hub_phase();
     a.skip_hubs = order != 0;   // the table push skips the high-degree vertices
@@ -2029,6 +2018,8 @@ extern "C" int excent_engine_set_hub_targets(excent_engine* e, int k) {
         cudaFuncSetAttribute(k_push<4, SRC_GATHER>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz);
         cudaFuncSetAttribute(k_push<4, SRC_HOT>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz);
         cudaFuncSetAttribute(k_push<4, SRC_HUBS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz);
+        cudaFuncSetAttribute(k_segments<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz);
+        cudaFuncSetAttribute(k_segments<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz);
         EX_CUDA(cudaGetLastError());
     }
     int occ = 0;
@@ -2050,20 +2041,31 @@ extern "C" int excent_engine_set_hub_order(excent_engine* e, int order) {
 // Every entry of the edge cache, in cache order, reduced into a scratch array
 // shaped like r: the scatter's ceiling on this graph's target distribution.
 template <int L>
-__global__ void k_scatter_probe(ull m, const int* cache, const int* hub_id, typename Lane<L>::T* out) {
+__global__ void __launch_bounds__(BLOCK) k_scatter_probe(ull m, const int* cache, const int* hub_id, int hub_k,
+                                                         typename Lane<L>::T* out) {
     typedef typename Lane<L>::T T;
+    T* hacc = hacc_init<T>(hub_k);
     T one;
     if constexpr (L == 1) one = 1.f; else one = make_float4(1.f, 1.f, 1.f, 0.f);
     const ull stride = (ull)gridDim.x * blockDim.x;
     const ull m4 = m / 4;
     const int4* c4 = reinterpret_cast<const int4*>(cache);
-    auto dec = [&](int u) { return u < 0 ? hub_id[u & HUB_MASK] : u; };
-    for (ull i = blockIdx.x * (ull)blockDim.x + threadIdx.x; i < m4; i += stride) {
-        const int4 q = ld_edge4(c4 + i);
-        red_add(out, dec(q.x), one); red_add(out, dec(q.y), one);
-        red_add(out, dec(q.z), one); red_add(out, dec(q.w), one);
+    ull i = blockIdx.x * (ull)blockDim.x + threadIdx.x;
+    for (; i + stride < m4; i += 2 * stride) {   // two 16-byte loads in flight per thread
+        const int4 q = ld_edge4(c4 + i), w = ld_edge4(c4 + i + stride);
+        scatter_one(out, q.x, one, hacc); scatter_one(out, q.y, one, hacc);
+        scatter_one(out, q.z, one, hacc); scatter_one(out, q.w, one, hacc);
+        scatter_one(out, w.x, one, hacc); scatter_one(out, w.y, one, hacc);
+        scatter_one(out, w.z, one, hacc); scatter_one(out, w.w, one, hacc);
     }
-    for (ull i = m4 * 4 + blockIdx.x * (ull)blockDim.x + threadIdx.x; i < m; i += stride) red_add(out, dec(cache[i]), one);
+    for (; i < m4; i += stride) {
+        const int4 q = ld_edge4(c4 + i);
+        scatter_one(out, q.x, one, hacc); scatter_one(out, q.y, one, hacc);
+        scatter_one(out, q.z, one, hacc); scatter_one(out, q.w, one, hacc);
+    }
+    for (ull j = m4 * 4 + blockIdx.x * (ull)blockDim.x + threadIdx.x; j < m; j += stride)
+        scatter_one(out, cache[j], one, hacc);
+    hacc_flush(hacc, out, hub_id, hub_k);
 }
 
 extern "C" int excent_engine_scatter_peak(excent_engine* e, double* entries_per_second) {
@@ -2078,10 +2080,18 @@ extern "C" int excent_engine_scatter_peak(excent_engine* e, double* entries_per_
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     float best = 0.f;
+    if (hub_smem(e)) {
+        cudaFuncSetAttribute(k_scatter_probe<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hub_smem(e));
+        cudaFuncSetAttribute(k_scatter_probe<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hub_smem(e));
+    }
     for (int rep = 0; rep < 4; rep++) {   // the first launch warms up; best of the other three
         cudaEventRecord(e0, e->s_main);
-        if (e->L == 1) k_scatter_probe<1><<<e->sms * 8, BLOCK, 0, e->s_main>>>(e->m, e->d_cache, e->d_hub_id, (float*)out);
-        else k_scatter_probe<4><<<e->sms * 8, BLOCK, 0, e->s_main>>>(e->m, e->d_cache, e->d_hub_id, (float4*)out);
+        if (e->L == 1)
+            k_scatter_probe<1><<<e->grid_push, BLOCK, hub_smem(e), e->s_main>>>(e->m, e->d_cache, e->d_hub_id, e->hub_k,
+                                                                               (float*)out);
+        else
+            k_scatter_probe<4><<<e->grid_push, BLOCK, hub_smem(e), e->s_main>>>(e->m, e->d_cache, e->d_hub_id, e->hub_k,
+                                                                               (float4*)out);
         cudaEventRecord(e1, e->s_main);
         cudaEventSynchronize(e1);
         float ms = 0.f;
