@@ -1360,9 +1360,8 @@ extern "C" int excent_engine_push_cached(excent_engine* e, const unsigned char* 
     EX_CUDA(cudaMemcpyAsync(e->d_wt_type, e->h_wt_type, e->nc, cudaMemcpyHostToDevice, e->s_main));
     EX_CUDA(cudaMemcpyAsync(e->d_wt_prefix, e->h_wt_prefix, ((size_t)e->nc + 1) * sizeof(unsigned),
                             cudaMemcpyHostToDevice, e->s_main));
-    PushArgs a = push_args(e, 0);
-    a.hot = e->hot_skip ? e->d_hot : nullptr;
-    // a high-degree order needs every chunk with work in the cache (the hub list spans the graph)
+    // a high-degree order needs every chunk with work in the cache (the hub list spans the graph);
+    // the hub list is built before the push arguments are taken, which point at it
     bool all_cached = true;
     for (int c = 0; c < e->nc; c++) all_cached &= cnt[2 * c] == 0 || mode[c] == 1;
     int order = 0;
@@ -1370,6 +1369,8 @@ extern "C" int excent_engine_push_cached(excent_engine* e, const unsigned char* 
         EX_TRY(ensure_hubv(e));
         order = effective_order(e);
     }
+    PushArgs a = push_args(e, 0);
+    a.hot = e->hot_skip ? e->d_hot : nullptr;
     if (order == 1) launch_push<SRC_HUBS>(e, a, e->grid_push, e->s_main);
     a.skip_hubs = order != 0;
     if (sweep_of(e)) {   // one launch per chunk, in chunk order

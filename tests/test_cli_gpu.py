@@ -134,18 +134,29 @@ def rmat16_cfg(tmp_path_factory):
 def test_error_no_looser_than_reference_binary_rmat16(rmat16_cfg, tmp_path, measure, mode):
     """Error against the FP64 oracle (L1 relative, max per-vertex, top-1000 overlap) of this
     repo's CLI against the reference binary's on the same R-MAT scale-16 file and flags.
-    Both are FP32 with atomics in a run-dependent order; the allowance for that is 5 % of
-    L1, 25 % of the max per-vertex error and 5 of the top 1000."""
+    Both add FP32 residuals with atomics in a run-dependent order (the reference's own Katz
+    L1 moved by 9 % between two runs here), so each side is the median of three runs; the
+    allowance is 5 % of L1, 25 % of the max per-vertex error and 5 of the top 1000."""
     if not os.path.exists(REF_CLI):
         pytest.skip("reference binary not built")
     p, n, idx, adj, env = rmat16_cfg
     args = [p, *env_args(env, measure), "--stream-ratio", "2", "--cache", "chunks"]
-    run(CLI, args + (["--device-loop"] if mode == "device-loop" else []) + ["--dump", str(tmp_path / "a")], tmp_path)
-    run(REF_CLI, args + ["--dump", str(tmp_path / "b")], tmp_path)
-    for k in (["pr", "katz", "ev"] if measure == "all" else ["pr"]):
-        ref_x = O.reference_solution(n, idx, adj, k, alpha=float(env["ALPHA"]))
-        a = O.compare(k, ref_x, np.fromfile(str(tmp_path / f"a.{k}.bin"), dtype=np.float32))
-        b = O.compare(k, ref_x, np.fromfile(str(tmp_path / f"b.{k}.bin"), dtype=np.float32))
+    kinds = ["pr", "katz", "ev"] if measure == "all" else ["pr"]
+    refs = {k: O.reference_solution(n, idx, adj, k, alpha=float(env["ALPHA"])) for k in kinds}
+    med = {}
+    for side, binary, extra in (("ours", CLI, ["--device-loop"] if mode == "device-loop" else []),
+                                ("reference", REF_CLI, [])):
+        runs = {k: [] for k in kinds}
+        for rep in range(3):
+            out = str(tmp_path / f"{side}{rep}")
+            run(binary, args + extra + ["--dump", out], tmp_path)
+            for k in kinds:
+                runs[k].append(O.compare(k, refs[k], np.fromfile(f"{out}.{k}.bin", dtype=np.float32)))
+        med[side] = {k: {q: float(np.median([r[q] for r in runs[k]])) for q in ("l1_rel", "max_abs", "top1000")}
+                     for k in kinds}
+    for k in kinds:
+        a, b = med["ours"][k], med["reference"][k]
+        print(k, "ours", a, "reference", b)
         assert a["l1_rel"] <= 1.05 * b["l1_rel"] + 1e-7, (k, a, b)
         assert a["max_abs"] <= 1.25 * b["max_abs"] + 1e-7, (k, a, b)
         assert a["top1000"] >= b["top1000"] - 5, (k, a, b)

@@ -543,6 +543,8 @@ def test_host_cache_zero_copy_solve(rmat16, measure, use_graph, resident):
     for mode in ("device", "host"):
         meas = X.measures(measure, **kw)
         eng = X.Engine(n, m, meas, v0, e)
+        eng.set_hub_order("first")    # the same pass order in both modes: this test is about where
+        eng.set_chunk_sweep(False)    # the lists are read from
         eng.upload_offsets(idx)
         if mode == "device":
             eng.reserve_cache(m)
