@@ -402,7 +402,7 @@ def run_ours(a, world, rank, local, dist):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded R-MAT, generated on the device)",
-        "config": {"workload": f"{measure} on R-MAT scale {scale} EF {ef} seed {seed}, fully HBM-cached",
+        "config": {"workload": f"{measure} on R-MAT scale {scale} EF {ef} seed {seed}", "cache": "fully HBM-cached",
                    "n": n, "m": m, "chunks": int(len(v0)), "measure": measure, "lambda1": lam,
                    "eps": [float(meas.eps[i]) for i in range(nm)], "passes_per_solve": passes[-1],
                    "pushed_per_solve": int(pushed / a.steps), "time_to_eps_ms": round(t / a.steps * 1e3, 3),
