@@ -235,6 +235,10 @@ class Engine:
         "auto": when the graph has more than one chunk."""
         call("excent_engine_set_chunk_sweep", self.h, -1 if on == "auto" else int(bool(on)))
 
+    def set_claim_tiles(self, tiles=0):
+        """Tiles of 32 items a push warp claims at a time (0: by the launch's size)."""
+        call("excent_engine_set_claim_tiles", self.h, int(tiles))
+
     def host_cache(self):
         """Pinned host memory for the entries past the edge cache (excent_engine_host_cache):
         returns (numpy int32 view to fill, first edge index)."""

@@ -33,20 +33,22 @@ enum { WT_NONE = 0, WT_LIST = 1, WT_RANGE = 2 };
 struct HubSeg {
     const int* nb;
     unsigned len;
-    unsigned tag;      // set to 1 once the segment is written; cleared by the warp that scatters it
+    unsigned pad;
     float4 p;
 };
 
 // The work queue of one push launch: tiles are claimed in batches from
-// `claim` (high 32 bits: batches claimed), long lists are queued as segments
-// at `tail` and taken from `head` by warps between batches; k_segments takes
-// the rest after the launch. Zeroed before every launch.
+// `claim` (high 32 bits: batches claimed); long lists are queued as segments
+// at `tail` and scattered by k_segments after the launch, one warp per
+// segment. Nothing inside k_push waits on another warp, and no counter is
+// contended by more than one atomic per warp and batch (claiming single
+// segments inside the launch, one CAS on a shared head per segment, was
+// measured ~100x slower on a 16.7M-vertex graph). Zeroed before every launch.
 struct PushQueue {
-    ull tail, head, claim, pad;
+    ull tail, claim, pad0, pad1;
 };
 static constexpr int TILE_BATCH = 32;           // at most this many tiles (of 32 items) per claim
 static constexpr unsigned SPIN_LIMIT = 1u << 24; // bounded polls of an mbarrier
-static constexpr long long WAIT_CYCLES = 2000000000ll;   // bounded wait for a reserved segment's tag (about a second)
 
 // Device control block: counters that live across kernels of one pass.
 struct Ctrl {
@@ -55,7 +57,7 @@ struct Ctrl {
     ull items;         // work items of the cached push in this pass
     int pass;          // passes that pushed so far
     int done;          // 1 once a snapshot found nothing pending (or max passes)
-    int err;           // 1: a hub queue overflowed; 2: a bounded wait for a queued segment gave up
+    int err;           // 1: a hub queue overflowed; 3: a bounded wait for a bulk copy gave up
     int pad0;
     double rsum[MAXM]; // FP64 sum |r| of the last snapshot
     unsigned hcount;   // hot pending list length
@@ -135,6 +137,7 @@ struct PushArgs {
     int skip_hubs;      // SRC_TABLE leaves the lists longer than HUB_MIN to SRC_HUBS
     int chunk;          // SRC_TABLE: only chunk `chunk`'s items (-1: every chunk's)
     int stage;          // SRC_CHUNK / SRC_GATHER: bulk-copy each tile's short lists into shared memory
+    int claim_tiles;    // tiles per claim; 0: up to TILE_BATCH, at least four claims per warp
     // lists past the device cache read in place from pinned host memory (zero copy)
     const int* hcache;   // entries [cache_edges, m), device-mapped
     ull cache_edges;
@@ -412,7 +415,7 @@ __global__ void k_plan(int nc, const int* cv0, int n, ull* cnt, const uint8_t* c
         ctrl->items = stop ? 0 : s_carry;
         ctrl->chunk_runs += s_runs;
         if (stop) ctrl->done = 1; else ctrl->pass = p + 1;
-        q0->tail = 0; q0->head = 0; q0->claim = 0;
+        q0->tail = 0; q0->claim = 0;
         ctrl->hotpend = 0;
         ctrl->ev_corr = ctrl->ev_dot;
         ctrl->ev_dot = 0;
@@ -499,59 +502,19 @@ __device__ __forceinline__ long long item_total(const PushArgs& a) {
     else return a.ctrl->hcount;
 }
 
-// Scatter queued segment i (reserved, so its tag is set soon): wait for the tag
-// (bounded), read it, clear the tag for the next launch, scatter. False if the
-// wait gave up (ctrl->err = 2).
+// Scatter queued segment i (written by an earlier launch on the stream).
 template <typename T>
-__device__ __forceinline__ bool scatter_segment(const PushArgs& a, T* r, T* hacc, int lane, ull i) {
-    int ok = 1;
-    if (lane == 0) {
-        const long long t0 = clock64();
-        while (!*(volatile unsigned*)&a.hubq[i].tag) {
-            if (clock64() - t0 > WAIT_CYCLES) { atomicExch(&a.ctrl->err, 2); ok = 0; break; }
-            __nanosleep(64);
-        }
-    }
-    if (!__shfl_sync(FULL, ok, 0)) return false;
-    __threadfence();
+__device__ __forceinline__ void scatter_segment(const PushArgs& a, T* r, T* hacc, int lane, ull i) {
     const HubSeg* hs = a.hubq + i;
-    const int* nb = (const int*)__ldcg((const unsigned long long*)&hs->nb);
-    const unsigned len = __ldcg(&hs->len);
-    const float4 p4 = __ldcg(&hs->p);
-    __syncwarp();
-    if (lane == 0) *(volatile unsigned*)&a.hubq[i].tag = 0u;   // the slot is clean for the next launch
+    const int* nb = hs->nb;
+    const unsigned len = hs->len;
+    const float4 p4 = hs->p;
     T p;
     if constexpr (sizeof(T) == sizeof(float)) p = p4.x; else p = p4;
     warp_scatter(r, nb, len, p, lane, hacc);
-    return true;
 }
 
-// Between batches of tiles: scatter the segments queued so far (claimed only
-// while the head is below the tail), so a long list's residual spreads soon
-// after it was taken, as a vertex's own scatter follows its take.
-template <typename T>
-__device__ __forceinline__ void help_segments(const PushArgs& a, T* r, T* hacc, int lane) {
-    for (;;) {
-        ull i = 0;
-        int got = 0;
-        if (lane == 0) {
-            ull h = *(volatile ull*)&a.q->head;
-            const ull t = *(volatile ull*)&a.q->tail;
-            while (h < t) {
-                const ull prev = atomicCAS(&a.q->head, h, h + 1);
-                if (prev == h) { got = 1; i = h; break; }
-                h = prev;
-            }
-        }
-        if (!__shfl_sync(FULL, got, 0)) return;
-        i = __shfl_sync(FULL, i, 0);
-        if (i >= a.hub_cap) continue;   // never written (the producer flagged the overflow)
-        if (!scatter_segment(a, r, hacc, lane, i)) return;
-    }
-}
-
-// Segments still queued when a push launch ends (reserved after the last
-// help, or never helped): one warp per segment, right after the launch.
+// The segments a push launch queued: one warp per segment, right after it.
 template <int L>
 __global__ void __launch_bounds__(BLOCK) k_segments(void* rv, PushArgs a) {
     typedef typename Lane<L>::T T;
@@ -560,8 +523,8 @@ __global__ void __launch_bounds__(BLOCK) k_segments(void* rv, PushArgs a) {
     const int lane = threadIdx.x & 31;
     const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    const ull head = a.q->head, tail = min(a.q->tail, a.hub_cap);
-    for (ull i = head + gw; i < tail; i += nwarps) scatter_segment(a, r, hacc, lane, i);
+    const ull tail = min(a.q->tail, a.hub_cap);
+    for (ull i = gw; i < tail; i += nwarps) scatter_segment(a, r, hacc, lane, i);
     hacc_flush(hacc, r, a.hub_id, a.hub_k);
 }
 
@@ -570,7 +533,7 @@ __global__ void __launch_bounds__(BLOCK) k_segments(void* rv, PushArgs a) {
 // src/excent.cu:109-112), then the warp dispatches by degree: lists of up to
 // HUB_MIN entries are scattered edge-balanced across the warp (lane j handles
 // the j-th entry of each 32-entry window of the tile's concatenated lists),
-// longer lists are queued as HUB_SEG-entry hub segments for k_hub. Residuals
+// longer lists are queued as HUB_SEG-entry segments for k_segments. Residuals
 // are added with red.global (a float4 reduction per entry carries every
 // measure of an `all` run), or in the block's shared hub-target slots.
 template <int L, int SRC>
@@ -598,7 +561,8 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
     const long long ntiles = total > first ? (total - first + 31) / 32 : 0;
     // claims of up to TILE_BATCH tiles, fewer when there are not four claims per warp
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    const long long per_claim = max(1ll, min((long long)TILE_BATCH, ntiles / (4 * nwarps)));
+    const long long per_claim =
+        a.claim_tiles > 0 ? a.claim_tiles : max(1ll, min((long long)TILE_BATCH, ntiles / (4 * nwarps)));
     const long long nbatch = (ntiles + per_claim - 1) / per_claim;
     ull pushed = 0, hpushed = 0, lanes = 0, taken = 0;
     for (;;) {
@@ -643,12 +607,10 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
                     HubSeg h;
                     h.nb = nb + (ull)s * HUB_SEG;
                     h.len = (unsigned)min((ull)HUB_SEG, deg - (ull)s * HUB_SEG);
-                    h.tag = 0;
+                    h.pad = 0;
                     if constexpr (L == 1) h.p = make_float4(p, 0.f, 0.f, 0.f); else h.p = p;
                     q[s] = h;
                 }
-                __threadfence();   // the segments are visible before they are marked written
-                for (unsigned s = 0; s < nseg; s++) *(volatile unsigned*)&q[s].tag = 1u;
             } else {
                 atomicExch(&a.ctrl->err, 1);
             }
@@ -717,9 +679,6 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
             __syncwarp();
         }
     }
-    __syncwarp();
-    // between batches, and once more when out of tiles: the segments queued so far
-    help_segments<T>(a, r, hacc, lane);
     if (batch >= nbatch) break;
     }
     pushed = warp_sum(pushed);
@@ -887,6 +846,7 @@ struct excent_engine {
     ull* d_hubv_cnt = nullptr;
     ull hubv_cap = 0;
     int hub_order = -1;      // high-degree lists: 0 in table order, 1 first, 2 last, -1 by the chunk count
+    int claim_tiles = 0;     // tiles per claim of k_push (0: by the launch's size)
     int sweep_mode = -1;     // cached pushes chunk by chunk (1), in one launch (0), -1 by the chunk count
     cudaGraphConditionalHandle* d_chunk_if = nullptr;  // per chunk: does this pass push it (graph IF nodes)
     std::vector<cudaGraphConditionalHandle> h_chunk_if;
@@ -935,6 +895,10 @@ static void invalidate_graph(excent_engine* e) {
 }
 
 static void scrub_queues(excent_engine* e);
+static const char* ctrl_error(int err) {
+    return err == 3 ? "a push kernel's wait for a bulk copy of its lists timed out"
+                    : "device capacity check failed (hub queue overflow)";
+}
 static int ensure_hubv(excent_engine* e);
 
 // Pass order. By default a graph cut into several chunks is pushed chunk by
@@ -1039,7 +1003,6 @@ static int engine_setup(excent_engine* e, int device, int n, ull m, const excent
     EX_CUDA(cudaMemset(e->d_cnt, 0, 2 * (size_t)nc * sizeof(ull)));
     EX_CUDA(cudaMemset(e->d_cmode, 0, (size_t)nc));
     EX_CUDA(cudaMemset(e->d_queue, 0, 3 * sizeof(PushQueue)));
-    EX_CUDA(cudaMemset(e->d_hubq[0], 0, e->hub_cap[0] * sizeof(HubSeg)));   // every tag clear
     int occ = 0;
     if (e->L == 1) EX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_push<1, SRC_TABLE>, BLOCK, 0));
     else EX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_push<4, SRC_TABLE>, BLOCK, 0));
@@ -1310,6 +1273,7 @@ static PushArgs push_args(excent_engine* e, int q) {
     a.hubq = e->d_hubq[q]; a.hub_cap = e->hub_cap[q]; a.q = e->d_queue + q; a.ctrl = e->d_ctrl;
     a.hub_id = e->d_hub_id; a.hub_k = e->hub_k;
     a.hubv = e->d_hubv; a.hubv_cnt = e->d_hubv_cnt; a.skip_hubs = 0; a.chunk = -1; a.stage = 0;
+    a.claim_tiles = e->claim_tiles;
     a.hcache = nullptr; a.cache_edges = e->cache_edges;
     if (e->h_hcache) cudaHostGetDevicePointer((void**)&a.hcache, e->h_hcache, 0);
     return a;
@@ -1587,8 +1551,7 @@ extern "C" int excent_engine_sync(excent_engine* e) {
     int err = 0;
     EX_CUDA(cudaMemcpy(&err, &e->d_ctrl->err, sizeof(int), cudaMemcpyDeviceToHost));
     if (err) scrub_queues(e);
-    if (err) EX_FAIL(EXCENT_ERR_STATE, "%s", err == 2 ? "a push kernel's wait for a queued segment timed out"
-                                                  : "device capacity check failed (hub queue overflow)");
+    if (err) EX_FAIL(EXCENT_ERR_STATE, "%s", ctrl_error(err));
     return EXCENT_OK;
 }
 
@@ -1750,7 +1713,7 @@ static int build_graph(excent_engine* e, double list_frac, int max_passes) {
 }
 
 // After a device-side failure, a segment may have been left marked written:
-// clear every queue and tag (and the flag) so no later launch reads one.
+// clear every queue (and the flag) so no later launch reads one.
 static void scrub_queues(excent_engine* e) {
     cudaDeviceSynchronize();
     for (int q = 0; q < 3; q++)
@@ -1874,8 +1837,7 @@ static int solve_impl(excent_engine* e, double list_frac, int max_passes, int us
     }
     EX_CUDA(cudaGetLastError());
     if (e->h_ctrl->err) scrub_queues(e);
-    if (e->h_ctrl->err) EX_FAIL(EXCENT_ERR_STATE, "%s", e->h_ctrl->err == 2 ? "a push kernel's wait for a queued segment timed out"
-                                                                        : "device capacity check failed (hub queue overflow)");
+    if (e->h_ctrl->err) EX_FAIL(EXCENT_ERR_STATE, "%s", ctrl_error(e->h_ctrl->err));
     return EXCENT_OK;
 }
 
@@ -2160,6 +2122,14 @@ extern "C" int excent_engine_set_chunk_sweep(excent_engine* e, int on) {
     EX_CUDA(cudaSetDevice(e->dev));
     invalidate_graph(e);
     e->sweep_mode = on < 0 ? -1 : (on != 0);
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_set_claim_tiles(excent_engine* e, int tiles) {
+    EX_CHECK_ARG(e && tiles >= 0 && tiles <= 1024, "tiles per claim must be 0 (by launch size) to 1024");
+    EX_CUDA(cudaSetDevice(e->dev));
+    invalidate_graph(e);
+    e->claim_tiles = tiles;
     return EXCENT_OK;
 }
 

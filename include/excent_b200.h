@@ -248,6 +248,10 @@ int excent_engine_set_hub_order(excent_engine* e, int order);
  * src/excent.cu:684-688), every chunk in one launch (0), or -1 (the default):
  * chunk by chunk when the graph has more than one chunk. */
 int excent_engine_set_chunk_sweep(excent_engine* e, int on);
+/* Tiles of 32 items a push warp claims at a time (1..1024), or 0 (the
+ * default): up to 32, at least four claims per warp. Fewer tiles per claim
+ * keep the items in flight closer together in table order. */
+int excent_engine_set_claim_tiles(excent_engine* e, int tiles);
 /* The scatter's ceiling on this graph: one reduction per edge-cache entry (in
  * cache order, to its target, into a scratch array shaped like the residuals),
  * best of three timed passes, as entries per second. Needs the whole graph in
