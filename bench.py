@@ -100,9 +100,12 @@ def parse():
                          "the chunks are swept one by one, else first)")
     ap.add_argument("--chunk-sweep", default="auto", choices=["auto", "on", "off"],
                     help="cached pushes one chunk per launch in chunk order (auto: when there are several chunks)")
+    ap.add_argument("--sweep-demand", type=float, default=0.5,
+                    help="with a chunk sweep: sweep only the passes whose pending entries reach this fraction of m "
+                         "(the others run as one launch); 0 sweeps every pass")
     ap.add_argument("--hub-targets", type=int, default=-1,
-                    help="shared-memory aggregation of the k highest-degree targets (0: off; -1: 16384 for "
-                         "one measure, 4096 for all)")
+                    help="shared-memory aggregation of the k highest-degree targets (0: off; -1: 4096 for all; "
+                         "for one measure 2048 with a chunk sweep, else 16384)")
     ap.add_argument("--ev-init", default="fp64", choices=["fp64", "reference"],
                     help="eigenvector initial residual from the FP64 lambda1 (default) or from lambda1 rounded to "
                          "float as the reference does")
@@ -244,6 +247,7 @@ def error_report(a, n, m, d_idx, d_adj, idx_np, adj_np, v0, e, eng, meas, measur
         eng2.set_hub_targets(min(4096, n))
         eng2.set_hub_order(a.hub_order)
         eng2.set_chunk_sweep({"auto": "auto", "on": True, "off": False}[a.chunk_sweep])
+        eng2.set_sweep_demand(a.sweep_demand)
         st = eng2.solve(list_frac=a.list_frac, max_passes=a.ref_passes)
         rep["like_for_like"] = {"ev_init": "lambda1 rounded to float", "ev_project": "off",
                                 "max_passes": a.ref_passes, "passes": st.passes,
@@ -312,10 +316,13 @@ def run_ours(a, world, rank, local, dist):
     eng.upload_device(d_idx, d_adj)
     if v1 is not None and a.ev_project == "on":
         eng.ev_project(v1)
-    hub_k = a.hub_targets if a.hub_targets >= 0 else min(16384 if nm == 1 else 4096, n)
+    # hub-target slots: fewer when each launch covers one chunk (a slot pays only with many adds per flush)
+    sweeping = a.chunk_sweep == "on" or (a.chunk_sweep == "auto" and len(v0) > 1)
+    hub_k = a.hub_targets if a.hub_targets >= 0 else min((2048 if sweeping else 16384) if nm == 1 else 4096, n)
     eng.set_hub_targets(hub_k)
     eng.set_hub_order(a.hub_order)
     eng.set_chunk_sweep({"auto": "auto", "on": True, "off": False}[a.chunk_sweep])
+    eng.set_sweep_demand(a.sweep_demand)
     use_graph = not a.no_graph
     for _ in range(a.warmup):
         s = eng.solve(list_frac=a.list_frac, use_graph=use_graph)
@@ -410,11 +417,11 @@ def run_ours(a, world, rank, local, dist):
                    "cuda_graph": use_graph, "parallelism": f"{world} independent replicas",
                    "ev_init": a.ev_init, "ev_project": a.ev_project if measure == "all" else None,
                    "hub_targets": hub_k, "list_frac": a.list_frac,
-                   "hub_order": a.hub_order, "chunk_sweep": a.chunk_sweep},
+                   "hub_order": a.hub_order, "chunk_sweep": a.chunk_sweep, "sweep_demand": a.sweep_demand},
         "e2e": {"value": round(e_pushed / te / 1e9, 4), "unit": "GTEPS", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": round(te / a.steps * 1e3, 3),
                 "wall_ms_per_step": round(te_wall / a.steps * 1e3, 3)},
-        "roofline": {"bound": "hbm", "kernel": "k_push + k_hub (one logical push per pass)",
+        "roofline": {"bound": "hbm", "kernel": "k_push + k_segments (one logical push: the takes, the short lists, then the queued long-list segments)",
                      "achieved": round(achieved, 1), "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": None,
                      "traffic_note": "not measured in this run; an ncu capture of one scale-24 solve of this "

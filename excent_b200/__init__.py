@@ -235,6 +235,10 @@ class Engine:
         "auto": when the graph has more than one chunk."""
         call("excent_engine_set_chunk_sweep", self.h, -1 if on == "auto" else int(bool(on)))
 
+    def set_sweep_demand(self, frac):
+        """Sweep (chunk by chunk) only the passes whose pending entries reach frac * m."""
+        call("excent_engine_set_sweep_demand", self.h, float(frac))
+
     def set_claim_tiles(self, tiles=0):
         """Tiles of 32 items a push warp claims at a time (0: by the launch's size)."""
         call("excent_engine_set_claim_tiles", self.h, int(tiles))

@@ -74,6 +74,7 @@ PROTOS = [
     ("excent_mtx_to_egr", C.c_int, [C.c_char_p, C.c_char_p, C.c_int, u64p]),
     ("excent_engine_set_chunk_sweep", C.c_int, [vp, C.c_int]),
     ("excent_engine_set_claim_tiles", C.c_int, [vp, C.c_int]),
+    ("excent_engine_set_sweep_demand", C.c_int, [vp, C.c_double]),
     ("excent_reduction_peak", C.c_int, [C.c_int, C.c_int, C.c_int, u64, f64p]),
     ("excent_engine_scatter_peak", C.c_int, [vp, f64p]),
     ("excent_engine_autotune", C.c_int, [vp, C.c_double, C.c_int, C.POINTER(Tune), C.POINTER(Tune), C.c_int,

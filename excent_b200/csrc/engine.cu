@@ -58,7 +58,7 @@ struct Ctrl {
     int pass;          // passes that pushed so far
     int done;          // 1 once a snapshot found nothing pending (or max passes)
     int err;           // 1: a hub queue overflowed; 3: a bounded wait for a bulk copy gave up
-    int pad0;
+    int sweep_pass;    // this pass is pushed chunk by chunk (set by k_plan)
     double rsum[MAXM]; // FP64 sum |r| of the last snapshot
     unsigned hcount;   // hot pending list length
     unsigned pad2;
@@ -354,7 +354,8 @@ __global__ void __launch_bounds__(BLOCK) k_snapshot(SnapArgs a) {
 // next snapshot accumulates into, and set the graph's loop condition.
 __global__ void k_plan(int nc, const int* cv0, int n, ull* cnt, const uint8_t* cmode, double list_frac, int max_passes,
                        uint8_t* wt_type, unsigned* wt_prefix, Ctrl* ctrl, PushQueue* q0, PassRec* log, int log_cap,
-                       cudaGraphConditionalHandle cond, int use_cond, const cudaGraphConditionalHandle* chunk_if) {
+                       cudaGraphConditionalHandle cond, int use_cond, const cudaGraphConditionalHandle* chunk_if,
+                       int sweep, ull sweep_min) {
     __shared__ ull s_pend, s_dem;
     __shared__ unsigned s_carry;
     __shared__ int s_nl, s_nr, s_runs;
@@ -370,6 +371,10 @@ __global__ void k_plan(int nc, const int* cv0, int n, ull* cnt, const uint8_t* c
     const ull pend = s_pend, dem = s_dem, hp = ctrl->hotpend;
     const int p = ctrl->pass;
     const bool stop = ctrl->done || p >= max_passes || (pend == 0 && hp == 0);
+    // a sweeping engine pushes a pass chunk by chunk while its demand is large, and in one
+    // launch once the pending entries fall below sweep_min (the per-chunk launches would
+    // then cost more than the in-pass ordering saves)
+    const bool sweep_pass = sweep && !stop && dem >= sweep_min;
     // work table, scanned in tiles of blockDim.x chunks
     for (int base = 0; base < nc; base += blockDim.x) {
         const int c = base + t;
@@ -395,8 +400,8 @@ __global__ void k_plan(int nc, const int* cv0, int n, ull* cnt, const uint8_t* c
         if (c < nc) {
             wt_type[c] = ty;
             wt_prefix[c + 1] = s_carry + s_scan[t];
-            if (chunk_if) cudaGraphSetConditional(chunk_if[c], items ? 1u : 0u);   // chunk sweep: launch it?
-            if (items) atomicAdd(&s_runs, 1);
+            if (chunk_if) cudaGraphSetConditional(chunk_if[c], sweep_pass && items ? 1u : 0u);   // launch it?
+            if (sweep_pass && items) atomicAdd(&s_runs, 1);
         }
         if (c == 0) wt_prefix[0] = 0;
         __syncthreads();
@@ -413,7 +418,10 @@ __global__ void k_plan(int nc, const int* cv0, int n, ull* cnt, const uint8_t* c
             R.n_list = s_nl; R.n_range = s_nr;
         }
         ctrl->items = stop ? 0 : s_carry;
-        ctrl->chunk_runs += s_runs;
+        // pushes launched this pass: one per chunk with items, or the one whole-table push
+        ctrl->chunk_runs += sweep_pass ? s_runs : (sweep && !stop && s_carry ? 1 : 0);
+        ctrl->sweep_pass = sweep_pass ? 1 : 0;
+        if (chunk_if) cudaGraphSetConditional(chunk_if[nc], sweep && !stop && !sweep_pass && s_carry ? 1u : 0u);
         if (stop) ctrl->done = 1; else ctrl->pass = p + 1;
         q0->tail = 0; q0->claim = 0;
         ctrl->hotpend = 0;
@@ -848,6 +856,7 @@ struct excent_engine {
     int hub_order = -1;      // high-degree lists: 0 in table order, 1 first, 2 last, -1 by the chunk count
     int claim_tiles = 0;     // tiles per claim of k_push (0: by the launch's size)
     int sweep_mode = -1;     // cached pushes chunk by chunk (1), in one launch (0), -1 by the chunk count
+    double sweep_frac = 0.5; // ... only in passes whose pending entries reach sweep_frac * m
     cudaGraphConditionalHandle* d_chunk_if = nullptr;  // per chunk: does this pass push it (graph IF nodes)
     std::vector<cudaGraphConditionalHandle> h_chunk_if;
     bool hubv_stale = true;
@@ -909,6 +918,8 @@ static int ensure_hubv(excent_engine* e);
 // lists first instead (measured: fewer entries and smaller errors than table
 // order there). Both can be set explicitly.
 static bool sweep_of(const excent_engine* e) { return e->sweep_mode >= 0 ? e->sweep_mode != 0 : e->nc > 1; }
+// A sweeping engine sweeps the passes whose pending entries reach this many.
+static ull sweep_min_entries(const excent_engine* e) { return (ull)(e->sweep_frac * (double)e->m); }
 static int order_of(const excent_engine* e) { return e->hub_order >= 0 ? e->hub_order : (sweep_of(e) ? 0 : 1); }
 // the order a pass can run: a high-degree order needs the listed high-degree vertices
 static int effective_order(const excent_engine* e);
@@ -1337,7 +1348,9 @@ extern "C" int excent_engine_push_cached(excent_engine* e, const unsigned char* 
     a.hot = e->hot_skip ? e->d_hot : nullptr;
     if (order == 1) launch_push<SRC_HUBS>(e, a, e->grid_push, e->s_main);
     a.skip_hubs = order != 0;
-    if (sweep_of(e)) {   // one launch per chunk, in chunk order
+    ull demand = 0;
+    for (int c = 0; c < e->nc; c++) demand += cnt[2 * c + 1];
+    if (sweep_of(e) && demand >= sweep_min_entries(e)) {   // one launch per chunk, in chunk order
         for (int c = 0; c < e->nc; c++) {
             const unsigned items = e->h_wt_prefix[c + 1] - e->h_wt_prefix[c];
             if (!items) continue;
@@ -1597,20 +1610,28 @@ static void pass_kernels(const excent_engine* e, int order, ull* fixed, ull* per
 // With ev, events are recorded between the kernels. chunk_body (a second
 // stream) is given while the pass is captured into a graph with a chunk
 // sweep: each chunk's launches then sit in an IF node that k_plan switches
-// off for chunks with nothing to push; e->h_chunk_if receives the handles.
-static cudaError_t enqueue_pass(excent_engine* e, double list_frac, int max_passes, cudaGraphConditionalHandle cond,
-                                int use_cond, cudaStream_t st, cudaEvent_t* ev = nullptr,
-                                cudaStream_t chunk_body = nullptr) {
+// on for chunks with something to push in a sweeping pass, and the
+// whole-table launch sits in one more IF node, switched on in the other
+// passes; e->h_chunk_if receives the nc + 1 handles.
+static void enqueue_plan(excent_engine* e, double list_frac, int max_passes, cudaGraphConditionalHandle cond,
+                         int use_cond, cudaStream_t st, cudaEvent_t* ev, bool use_if) {
     if (ev) cudaEventRecord(ev[0], st);
     launch_snapshot(e, false, st);
     if (ev) cudaEventRecord(ev[1], st);
-    const bool use_if = chunk_body && sweep_of(e);
     k_plan<<<1, 1024, 0, st>>>(e->nc, e->d_cv0, e->n, e->d_cnt, e->d_cmode, list_frac, max_passes, e->d_wt_type,
                                e->d_wt_prefix, e->d_ctrl, e->d_queue, e->d_log, e->log_cap, cond, use_cond,
-                               use_if ? e->d_chunk_if : nullptr);
+                               use_if ? e->d_chunk_if : nullptr, sweep_of(e) ? 1 : 0, sweep_min_entries(e));
     e->launches++;
     if (ev) cudaEventRecord(ev[2], st);
+}
+
+// The pushes of a pass. sweep_pass: whether k_plan chose a chunk-by-chunk pass
+// (known to the host-driven loop, which reads it back first); ignored while
+// capturing with IF nodes, which hold both forms.
+static cudaError_t enqueue_push(excent_engine* e, cudaStream_t st, cudaEvent_t* ev, cudaStream_t chunk_body,
+                                bool sweep_pass) {
     PushArgs a = push_args(e, 0);
+    const bool use_if = chunk_body && sweep_of(e);
     // high-degree order: 1 = the lists longer than HUB_MIN first, so their (large) share of the
     // pass's residual reaches every other vertex before that vertex is taken; 2 = last, so they
     // collect the pass's residual and push it once; 0 = in table order with the rest
@@ -1637,24 +1658,31 @@ static cudaError_t enqueue_pass(excent_engine* e, double list_frac, int max_pass
         }
         e->launches += 2;
     };
+    // one launch under an IF node (c = -1: the whole table)
+    auto guarded = [&](int c) -> cudaError_t {
+        a.chunk = c;
+        cudaError_t rc = open_if(st, chunk_body, &e->h_chunk_if[c >= 0 ? c : e->nc]);
+        if (rc != cudaSuccess) return rc;
+        table(chunk_body);
+        rc = close_if(chunk_body);
+        a.chunk = -1;
+        return rc;
+    };
     if (order == 1) hub_phase();
     a.skip_hubs = order != 0;   // the table push skips the high-degree vertices
-    if (sweep_of(e)) {
+    if (use_if) {
         // chunk by chunk: each chunk's push (with its long lists) completes before the next
-        // chunk's vertices are taken, so they see everything pushed so far
+        // chunk's vertices are taken, so they see everything pushed so far; or the whole table
+        for (int c = 0; c < e->nc; c++) {
+            const cudaError_t rc = guarded(c);
+            if (rc != cudaSuccess) return rc;
+        }
+        const cudaError_t rc = guarded(-1);
+        if (rc != cudaSuccess) return rc;
+    } else if (sweep_of(e) && sweep_pass) {
         for (int c = 0; c < e->nc; c++) {
             a.chunk = c;
-            cudaStream_t s = st;
-            if (use_if) {
-                const cudaError_t rc = open_if(st, chunk_body, &e->h_chunk_if[c]);
-                if (rc != cudaSuccess) return rc;
-                s = chunk_body;
-            }
-            table(s);
-            if (use_if) {
-                const cudaError_t rc = close_if(chunk_body);
-                if (rc != cudaSuccess) return rc;
-            }
+            table(st);
         }
         a.chunk = -1;
     } else {
@@ -1667,11 +1695,18 @@ static cudaError_t enqueue_pass(excent_engine* e, double list_frac, int max_pass
     return cudaGetLastError();
 }
 
+static cudaError_t enqueue_pass(excent_engine* e, double list_frac, int max_passes, cudaGraphConditionalHandle cond,
+                                int use_cond, cudaStream_t st, cudaStream_t chunk_body) {
+    enqueue_plan(e, list_frac, max_passes, cond, use_cond, st, nullptr, chunk_body && sweep_of(e));
+    return enqueue_push(e, st, nullptr, chunk_body, true);
+}
+
 static int build_graph(excent_engine* e, double list_frac, int max_passes) {
     if (e->gexec && e->graph_max_passes == max_passes && e->graph_list_frac == list_frac) return EXCENT_OK;
     invalidate_graph(e);
-    if (sweep_of(e) && !e->d_chunk_if) EX_ALLOC(e->d_chunk_if, (size_t)e->nc * sizeof(cudaGraphConditionalHandle));
-    e->h_chunk_if.assign(e->nc, 0);
+    if (sweep_of(e) && !e->d_chunk_if)
+        EX_ALLOC(e->d_chunk_if, (size_t)(e->nc + 1) * sizeof(cudaGraphConditionalHandle));
+    e->h_chunk_if.assign(e->nc + 1, 0);
     cudaGraph_t g;
     EX_CUDA(cudaGraphCreate(&g, 0));
     cudaGraphConditionalHandle h;
@@ -1690,7 +1725,7 @@ static int build_graph(excent_engine* e, double list_frac, int max_passes) {
     EX_CUDA(cudaStreamCreateWithFlags(&cb, cudaStreamNonBlocking));
     EX_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     const ull before = e->launches;
-    const cudaError_t pe = enqueue_pass(e, list_frac, max_passes, h, 1, cs, nullptr, sweep_of(e) ? cb : nullptr);
+    const cudaError_t pe = enqueue_pass(e, list_frac, max_passes, h, 1, cs, sweep_of(e) ? cb : nullptr);
     e->launches = before;
     cudaGraph_t captured;
     const cudaError_t ce = cudaStreamEndCapture(cs, &captured);
@@ -1702,7 +1737,7 @@ static int build_graph(excent_engine* e, double list_frac, int max_passes) {
         EX_CUDA(pe != cudaSuccess ? pe : ce);
     }
     if (sweep_of(e))
-        EX_CUDA(cudaMemcpy(e->d_chunk_if, e->h_chunk_if.data(), (size_t)e->nc * sizeof(cudaGraphConditionalHandle),
+        EX_CUDA(cudaMemcpy(e->d_chunk_if, e->h_chunk_if.data(), (size_t)(e->nc + 1) * sizeof(cudaGraphConditionalHandle),
                            cudaMemcpyHostToDevice));
     const cudaError_t ie = cudaGraphInstantiate(&e->gexec, g, 0);
     if (ie != cudaSuccess) { cudaGraphDestroy(g); e->gexec = nullptr; EX_CUDA(ie); }
@@ -1820,11 +1855,16 @@ static int solve_impl(excent_engine* e, double list_frac, int max_passes, int us
         pass_kernels(e, effective_order(e), &fixed, &per_chunk);
         e->launches += fixed * (e->h_ctrl->pass + 1) + per_chunk * e->h_ctrl->chunk_runs;
     } else {
+        // snapshot and plan, read the plan back (one sync per pass), then the pushes it chose
         for (int p = 0; p <= max_passes; p++) {
-            EX_CUDA(enqueue_pass(e, list_frac, max_passes, 0, 0, e->s_main, e->prof ? e->ev : nullptr));
+            cudaEvent_t* ev = e->prof ? e->ev : nullptr;
+            enqueue_plan(e, list_frac, max_passes, 0, 0, e->s_main, ev, false);
             EX_CUDA(cudaMemcpyAsync(e->h_ctrl, e->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, e->s_main));
             EX_CUDA(cudaStreamSynchronize(e->s_main));
-            if (e->prof && !e->h_ctrl->done) {
+            if (e->h_ctrl->done) break;
+            EX_CUDA(enqueue_push(e, e->s_main, ev, nullptr, e->h_ctrl->sweep_pass != 0));
+            if (ev) {
+                EX_CUDA(cudaStreamSynchronize(e->s_main));
                 for (int k = 0; k < 4; k++) {
                     float ms = 0;
                     EX_CUDA(cudaEventElapsedTime(&ms, e->ev[k], e->ev[k + 1]));
@@ -1832,7 +1872,6 @@ static int solve_impl(excent_engine* e, double list_frac, int max_passes, int us
                 }
                 e->prof_passes++;
             }
-            if (e->h_ctrl->done) break;
         }
     }
     EX_CUDA(cudaGetLastError());
@@ -2077,10 +2116,13 @@ extern "C" int excent_engine_autotune(excent_engine* e, double list_frac, int ma
     EX_CHECK_ARG(e && best, "null argument");
     EX_CHECK_ARG(e->d_cache && e->cache_edges == e->m, "autotuning needs the whole graph in the edge cache");
     EX_CUDA(cudaSetDevice(e->dev));
-    const int k_hi = std::min(e->n, e->L == 1 ? 16384 : 4096), k_lo = std::min(e->n, e->L == 1 ? 4096 : 2048);
+    // hub-target slots: a chunk-by-chunk pass flushes them once per chunk, so it measured
+    // best with fewer slots (2048 for one measure) than a one-launch pass (16384)
+    auto k = [&](int want) { return std::min(e->n, want); };
+    const bool one = e->L == 1;
     const excent_tune cands[] = {
-        {k_hi, 0, 1, 0.0}, {k_lo, 0, 1, 0.0}, {0, 0, 1, 0.0},   // table order, chunk by chunk
-        {k_hi, 1, 0, 0.0}, {k_lo, 1, 0, 0.0}, {0, 1, 0, 0.0},   // high-degree lists first, one launch
+        {k(2048), 0, 1, 0.0}, {k(one ? 16384 : 4096), 0, 1, 0.0}, {k(512), 0, 1, 0.0},   // table order, swept
+        {k(one ? 16384 : 4096), 1, 0, 0.0}, {k(one ? 4096 : 2048), 1, 0, 0.0}, {0, 1, 0, 0.0},   // lists first
     };
     const int nc = (int)(sizeof cands / sizeof cands[0]);
     cudaEvent_t t0, t1;
@@ -2122,6 +2164,14 @@ extern "C" int excent_engine_set_chunk_sweep(excent_engine* e, int on) {
     EX_CUDA(cudaSetDevice(e->dev));
     invalidate_graph(e);
     e->sweep_mode = on < 0 ? -1 : (on != 0);
+    return EXCENT_OK;
+}
+
+extern "C" int excent_engine_set_sweep_demand(excent_engine* e, double frac) {
+    EX_CHECK_ARG(e && frac >= 0.0 && frac <= 1e6, "sweep demand must be a fraction of m >= 0");
+    EX_CUDA(cudaSetDevice(e->dev));
+    invalidate_graph(e);
+    e->sweep_frac = frac;
     return EXCENT_OK;
 }
 

@@ -53,6 +53,7 @@ struct Options {
     int hub_order = -1;        // the high-degree lists 0 in table order, 1 first, 2 last, -1 by the chunk count
     std::string host_cache = "off";   // pinned: entries past the HBM cache read in place from pinned host memory
     int chunk_sweep = -1;      // cached pushes one chunk per launch (1), in one launch (0), -1 by the chunk count
+    double sweep_demand = 0.5; // ... in the passes whose pending entries reach this fraction of m
 };
 
 static const char* USAGE =
@@ -130,6 +131,12 @@ static int parse_options(int argc, char** argv, Options& o) {
                     return 1;
                 }
                 o.chunk_sweep = !strcmp(v, "auto") ? -1 : !strcmp(v, "on");
+            }
+        }
+        else if (a == "--sweep-demand") {
+            if ((ok = next(v))) {
+                o.sweep_demand = atof(v);
+                if (!(o.sweep_demand >= 0.0)) { fprintf(stderr, "--sweep-demand must be a fraction >= 0\n"); return 1; }
             }
         }
         else if (a == "--hub-order") {
@@ -464,13 +471,17 @@ private:
                 n_resident_--;
             for (int c = 0; c < n_resident_; c++) { resident_[c] = 1; resident_entries_ += ch_[c].edges(); }
             if (n_resident_ > 0) {   // shared-memory sums for the top-degree targets of cached pushes
-                const int k = o_.hub_targets < 0 ? std::min(M_.nm == 1 ? 16384 : 4096, g_.n) : o_.hub_targets;
+                // fewer slots when each launch covers one chunk: a slot pays only with many adds per flush
+                const bool sweeping = o_.chunk_sweep == 1 || (o_.chunk_sweep < 0 && ch_.size() > 1);
+                const int k_auto = M_.nm == 1 ? (sweeping ? 2048 : 16384) : 4096;
+                const int k = o_.hub_targets < 0 ? std::min(k_auto, g_.n) : o_.hub_targets;
                 if (k > 0 && excent_engine_set_hub_targets(e_, k) != EXCENT_OK)   // an optimisation: go on without it
                     fprintf(stderr, "excent: hub targets off (%s)\n", excent_last_error());
             }
         }
         RT_CK(excent_engine_set_hub_order(e_, o_.hub_order));
         RT_CK(excent_engine_set_chunk_sweep(e_, o_.chunk_sweep));
+        RT_CK(excent_engine_set_sweep_demand(e_, o_.sweep_demand));
         hot_mode_ = cache_mode_ == "hot";
         if (hot_mode_) return setup_degree_cache(reserve);
         return 0;

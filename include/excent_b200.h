@@ -248,6 +248,12 @@ int excent_engine_set_hub_order(excent_engine* e, int order);
  * src/excent.cu:684-688), every chunk in one launch (0), or -1 (the default):
  * chunk by chunk when the graph has more than one chunk. */
 int excent_engine_set_chunk_sweep(excent_engine* e, int on);
+/* A sweeping engine (excent_engine_set_chunk_sweep) pushes a pass chunk by
+ * chunk only while the pass's pending entries (the sum of the pending
+ * vertices' degrees) reach frac * m; a pass below that is pushed in one
+ * launch, whose per-chunk launches would cost more than the ordering saves.
+ * 0 sweeps every pass. Applies to the device solve and to cached pushes. */
+int excent_engine_set_sweep_demand(excent_engine* e, double frac);
 /* Tiles of 32 items a push warp claims at a time (1..1024), or 0 (the
  * default): up to 32, at least four claims per warp. Fewer tiles per claim
  * keep the items in flight closer together in table order. */

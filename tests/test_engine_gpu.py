@@ -455,6 +455,46 @@ def test_chunk_sweep_matches_one_launch(rmat16, measure, use_graph, order):
 
 
 @pytest.mark.parametrize("measure", ["pr", "all"])
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_sweep_demand_threshold(rmat16, measure, use_graph):
+    """A sweeping engine with a demand threshold sweeps only the passes whose
+    pending entries reach frac * m and pushes the others in one launch: the
+    same fixed point, and a launch count between the one-launch solve's and the
+    every-pass sweep's. A threshold above any demand launches like no sweep."""
+    n, idx, adj = rmat16
+    m = len(adj)
+    par = O.params(n, idx, adj)
+    kw = dict(alpha=0.9 / par["_lambda"], lam=par["_lambda"], eps_katz=1e-5, eps_ev=1e-5) if measure == "all" else {}
+    names = ["pr", "katz", "ev"] if measure == "all" else ["pr"]
+    res = {}
+    for tag, sweep, frac in [("one", False, 0.0), ("all", True, 0.0), ("some", True, 0.3), ("none", True, 1e6)]:
+        meas = X.measures(measure, **kw)
+        eng = make_engine(n, idx, adj, meas, cap=m // 7 + 1)
+        eng.set_hub_order("table")
+        eng.set_chunk_sweep(sweep)
+        eng.set_sweep_demand(frac)
+        l0 = eng.launches()
+        st = eng.solve(use_graph=use_graph)
+        res[(tag, "launches")] = eng.launches() - l0
+        _, plog = eng.stats(with_log=True)
+        res[(tag, "demand")] = [int(p.demand) for p in plog]
+        for i, k in enumerate(names):
+            r = eng.read(i, residual=True)
+            assert np.all(np.abs(r) <= np.float32(meas.eps[i])), (tag, k)
+            ref = O.reference_solution(n, idx, adj, k, alpha=kw.get("alpha"))
+            res[(tag, k)] = O.compare(k, ref, eng.read(i))
+        eng.close()
+    print(res)
+    d = res[("some", "demand")]
+    assert max(d) >= 0.3 * m > min(d)   # both kinds of pass occur
+    for k in names:
+        for tag in ("some", "none"):
+            assert res[(tag, k)]["l1_rel"] <= 1.25 * res[("one", k)]["l1_rel"] + 3e-5, (tag, k, res)
+    assert res[("one", "launches")] <= res[("some", "launches")] + 2 < res[("all", "launches")] + 2
+    assert abs(res[("none", "launches")] - res[("one", "launches")]) <= 2
+
+
+@pytest.mark.parametrize("measure", ["pr", "all"])
 @pytest.mark.parametrize("k", [1, 64, 2048])
 @pytest.mark.parametrize("sweep", [False, True])
 def test_hub_targets_match_plain_push(rmat16, measure, k, sweep):
