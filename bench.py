@@ -671,8 +671,9 @@ def run_adjoint(a, world, rank, local, dist):
             "grad_t_rel_err_vs_fp64_oracle": rel_or_t, "katz_beta_grad_rel_err_vs_fp64_oracle": rel_katz}
 
 
-def cpu_sample(n, idx, adj, meas, measure, lam, max_edges):
-    """The oracle's CPU port of the engine, bounded to about max_edges pushed entries."""
+def cpu_sample(n, idx, adj, meas, measure, lam, max_edges, threads=None):
+    """The oracle's CPU port of the engine, bounded to about max_edges pushed entries
+    (threads: OpenMP threads, default every host core)."""
     import oracle as O
     kinds = ["pr", "katz", "ev"] if measure == "all" else [measure]
     kw = {}
@@ -681,7 +682,7 @@ def cpu_sample(n, idx, adj, meas, measure, lam, max_edges):
     cv0 = np.ascontiguousarray(O.plan_chunks(idx, O.chunk_cap(len(adj)))[:, 0].astype(np.int32))
     t0 = time.perf_counter()
     _, _, passes, pushed = O.delta_push(n, idx, np.ascontiguousarray(adj), kinds, cv0=cv0, eps_pr=float(meas.eps[0]),
-                                        max_edges=max_edges, threads=os.cpu_count(), **kw)
+                                        max_edges=max_edges, threads=threads or os.cpu_count(), **kw)
     return pushed, passes, time.perf_counter() - t0
 
 
@@ -915,11 +916,19 @@ def run_ooc(a, world, rank, local, dist):
         shutil.rmtree(d, ignore_errors=True)
 
 
+def one_core(n, idx, adj, meas, measure, lam):
+    """The same port on one host core: its first pass (every vertex pending)."""
+    p1, passes, t1 = cpu_sample(n, idx, adj, meas, measure, lam, max_edges=1, threads=1)
+    return {"value": round(p1 / t1 / 1e9, 5), "unit": "GTEPS", "cores": 1,
+            "sample": f"{passes} pass(es), {p1} entries pushed in {t1:.2f}s, one thread"}
+
+
 def cpu_baseline(n, idx, adj, meas, measure, lam):
     pushed, passes, t = cpu_sample(n, idx, adj, meas, measure, lam, max_edges=len(adj))
     return {"value": round(pushed / t / 1e9, 5), "unit": "GTEPS", "cores": os.cpu_count(), "kind": "port",
             "sample": f"first {passes} pass(es) of the same solve ({pushed} entries pushed in {t:.2f}s) by the "
-                      "OpenMP CPU port of the reference engine (oracle/oracle.c)"}
+                      "OpenMP CPU port of the reference engine (oracle/oracle.c)",
+            "one_core": one_core(n, idx, adj, meas, measure, lam)}
 
 
 def run_reference(a, world, rank):
@@ -959,7 +968,8 @@ def run_reference(a, world, rank):
             "config": {"workload": f"{measure} on R-MAT scale {scale} EF {ef} seed {seed}", "n": n, "m": len(adj)},
             "cpu_baseline": {"value": round(v, 5), "unit": "GTEPS", "cores": os.cpu_count(), "kind": "port",
                              "sample": "pass 0 of the solve (every vertex pending) per step; the reference has "
-                                       "no CPU engine, so this is the OpenMP port in oracle/oracle.c"},
+                                       "no CPU engine, so this is the OpenMP port in oracle/oracle.c",
+                             "one_core": one_core(n, idx, adj, meas, measure, lam)},
             "e2e": {"value": round(v, 5), "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 

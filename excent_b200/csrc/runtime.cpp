@@ -110,6 +110,15 @@ static int parse_options(int argc, char** argv, Options& o) {
         else if (a == "--device") { if ((ok = next(v))) o.device = atoi(v); }
         else if (a == "--gpu-budget-gb") { if ((ok = next(v))) o.budget_gb = atof(v); }
         else if (a == "--device-loop") o.device_loop = true;
+        else if (a == "--ev-init") {
+            if ((ok = next(v))) {
+                if (strcmp(v, "fp64") && strcmp(v, "reference")) {
+                    fprintf(stderr, "--ev-init must be fp64 or reference\n");
+                    return 1;
+                }
+                o.ev_init_fp64 = !strcmp(v, "fp64");
+            }
+        }
         else if (a == "--hub-targets") {
             if ((ok = next(v))) {
                 if (!strcmp(v, "auto")) o.hub_targets = -1;

@@ -331,6 +331,18 @@ def test_cli_graph_line_matches_reference(extra, rmat14_files):
         assert g1 == g2
 
 
+@pytest.mark.parametrize("args,msg", [
+    (["--ev-init", "fp32"], "--ev-init must be fp64 or reference"),
+    (["--chunk-sweep", "maybe"], "--chunk-sweep must be on, off or auto"),
+    (["--sweep-demand", "-1"], "--sweep-demand must be a fraction >= 0"),
+    (["--host-cache", "mapped"], "--host-cache must be pinned or off"),
+])
+def test_cli_own_option_errors(args, msg):
+    """This CLI's own options (beside the reference's) reject bad values before any work."""
+    r = subprocess.run([CLI, SAMPLE, "--measure", "pr", *args], capture_output=True, text=True)
+    assert r.returncode == 1 and msg in r.stderr, r.stderr
+
+
 def test_cli_bad_file_is_an_error(tmp_path):
     p = tmp_path / "t.egr"
     p.write_bytes(np.array([100, 50], dtype="<i4").tobytes())
