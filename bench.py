@@ -49,6 +49,14 @@ CONFIGS = {
 
 T_START = time.perf_counter()
 
+# DRAM bytes (read + write) of the push kernels per solve, GB, from the ncu captures summarised in
+# profiles/ (dram__bytes_read.sum + dram__bytes_write.sum, one pass per launch, three solves)
+TRAFFIC_CAPTURES = {
+    ("cached-all", 24): (302.4, "GB per solve: k_push 113.7 + k_segments 188.7, ncu over three solves of "
+                                "`bench.py --steps 1 --warmup 0 --no-cpu-baseline --errors off --no-graph` "
+                                "(profiles/traffic_all_rmat24.md); `achieved` and `traffic` are both per solve"),
+}
+
 
 def log(msg):
     """Progress on stderr (the JSON line alone goes to stdout)."""
@@ -100,6 +108,8 @@ def parse():
                          "the chunks are swept one by one, else first)")
     ap.add_argument("--chunk-sweep", default="auto", choices=["auto", "on", "off"],
                     help="cached pushes one chunk per launch in chunk order (auto: when there are several chunks)")
+    ap.add_argument("--error-runs", type=int, default=3,
+                    help="solves per error figure (each engine's figure is the median over them)")
     ap.add_argument("--sweep-demand", type=float, default=0.5,
                     help="with a chunk sweep: sweep only the passes whose pending entries reach this fraction of m "
                          "(the others run as one launch); 0 sweeps every pass")
@@ -223,12 +233,24 @@ def fp64_solutions(n, d_idx, d_adj, kinds, alpha, device):
     return out
 
 
+def median_errors(runs):
+    """Per measure and metric, the median over runs (each a {measure: error_vs_fp64} dict), with the
+    L1 range of the runs."""
+    out = {}
+    for k in runs[0]:
+        out[k] = {q: float(np.median([r[k][q] for r in runs])) for q in ("l1_rel", "max_abs", "top1000")}
+        out[k]["l1_range"] = [min(r[k]["l1_rel"] for r in runs), max(r[k]["l1_rel"] for r in runs)]
+        out[k]["max_abs_range"] = [min(r[k]["max_abs"] for r in runs), max(r[k]["max_abs"] for r in runs)]
+    return out
+
+
 def error_report(a, n, m, d_idx, d_adj, idx_np, adj_np, v0, e, eng, meas, measure, lam, device):
     """Error of this engine's results against the FP64 oracle solution, in the timed configuration and
     like for like with the reference engine (eigenvector initial residual from lambda1 rounded to float,
     no FP64 eigenvector step, the same pass cap), beside the reference engine's own error: its CLI
     (src/excent.cu built from source) on the same EGR file and constants, results through --dump
-    (src/excent.cu:763-777)."""
+    (src/excent.cu:763-777). Both engines add FP32 residuals with atomics in a run-dependent order,
+    so each figure is the median of --error-runs solves, with the range of their L1 errors."""
     import shutil
 
     import excent_b200 as X
@@ -238,7 +260,12 @@ def error_report(a, n, m, d_idx, d_adj, idx_np, adj_np, v0, e, eng, meas, measur
     rep = {"oracle": "FP64 Jacobi (PageRank, Katz) and power iteration (eigenvector) on the device to a relative "
                      "change of 1e-9 (tools/centrality_reference.cu:184-214); the eigenvector is compared as a "
                      "unit vector with its sign fixed by its sum",
-           "timed_config": {k: error_vs_fp64(k, ref[k], eng.read(i)) for i, k in enumerate(kinds)}}
+           "runs_per_figure": a.error_runs}
+    ours = []
+    for _ in range(a.error_runs):
+        eng.solve(list_frac=a.list_frac, use_graph=not a.no_graph)
+        ours.append({k: error_vs_fp64(k, ref[k], eng.read(i)) for i, k in enumerate(kinds)})
+    rep["timed_config"] = median_errors(ours)
     if measure == "all":
         meas_l = X.measures("all", alpha=alpha, beta=1.0, lam=lam, eps_pr=1e-2, eps_katz=1e-6, eps_ev=1e-6,
                             ev_init_fp64=False)
@@ -248,10 +275,12 @@ def error_report(a, n, m, d_idx, d_adj, idx_np, adj_np, v0, e, eng, meas, measur
         eng2.set_hub_order(a.hub_order)
         eng2.set_chunk_sweep({"auto": "auto", "on": True, "off": False}[a.chunk_sweep])
         eng2.set_sweep_demand(a.sweep_demand)
-        st = eng2.solve(list_frac=a.list_frac, max_passes=a.ref_passes)
+        lfl = []
+        for _ in range(a.error_runs):
+            st = eng2.solve(list_frac=a.list_frac, max_passes=a.ref_passes)
+            lfl.append({k: error_vs_fp64(k, ref[k], eng2.read(i)) for i, k in enumerate(kinds)})
         rep["like_for_like"] = {"ev_init": "lambda1 rounded to float", "ev_project": "off",
-                                "max_passes": a.ref_passes, "passes": st.passes,
-                                **{k: error_vs_fp64(k, ref[k], eng2.read(i)) for i, k in enumerate(kinds)}}
+                                "max_passes": a.ref_passes, "passes": st.passes, **median_errors(lfl)}
         eng2.close()
     ref_bin = os.path.join(ROOT, "oracle", "_ref", "excent")
     if not os.path.exists(ref_bin):
@@ -266,18 +295,20 @@ def error_report(a, n, m, d_idx, d_adj, idx_np, adj_np, v0, e, eng, meas, measur
         if measure == "all":
             args += ["--alpha", "%.9g" % alpha, "--beta", "1", "--lambda", "%.17g" % lam, "--eps-katz", "1e-6",
                      "--eps-ev", "1e-6"]
-        r = subprocess.run([ref_bin, *args], capture_output=True, text=True, timeout=1800,
-                           env=dict(os.environ, HOME=d))
-        if r.returncode != 0:
-            rep["reference_engine"] = {"error": (r.stderr or r.stdout)[-300:]}
-            return rep
         import re
-        mp = re.search(r"^passes (\d+)", r.stdout, re.M)
-        got = {"args": " ".join(args[1:]).replace(d, "<tmp>"), "passes": int(mp.group(1)) if mp else None}
-        for k in kinds:
-            x = np.fromfile(os.path.join(d, f"out.{k}.bin"), dtype=np.float32)
-            got[k] = error_vs_fp64(k, ref[k], x)
-        rep["reference_engine"] = got
+        runs, passes = [], []
+        for _ in range(a.error_runs):
+            r = subprocess.run([ref_bin, *args], capture_output=True, text=True, timeout=1800,
+                               env=dict(os.environ, HOME=d))
+            if r.returncode != 0:
+                rep["reference_engine"] = {"error": (r.stderr or r.stdout)[-300:]}
+                return rep
+            mp = re.search(r"^passes (\d+)", r.stdout, re.M)
+            passes.append(int(mp.group(1)) if mp else None)
+            runs.append({k: error_vs_fp64(k, ref[k], np.fromfile(os.path.join(d, f"out.{k}.bin"), dtype=np.float32))
+                         for k in kinds})
+        rep["reference_engine"] = {"args": " ".join(args[1:]).replace(d, "<tmp>"), "passes": passes,
+                                   **median_errors(runs)}
     finally:
         shutil.rmtree(d, ignore_errors=True)
     return rep
@@ -396,6 +427,11 @@ def run_ours(a, world, rank, local, dist):
     red_peak = eng.scatter_peak()
     red_uniform = X.reduction_peak(n, vec4=nm > 1, device=local)
     red_achieved = ep / t_push if t_push > 0 else 0.0
+    # DRAM traffic of the push kernels per solve, from an ncu capture of this workload (ncu cannot
+    # run inside the timed process); other workloads: not captured
+    traffic, traffic_note = None, "no ncu capture of this workload"
+    if (a.config, scale) in TRAFFIC_CAPTURES:
+        traffic, traffic_note = TRAFFIC_CAPTURES[(a.config, scale)]
     result = {
         "metric": "GTEPS (adjacency entries pushed per second, solve to eps)",
         "value": round(value, 4),
@@ -423,10 +459,8 @@ def run_ours(a, world, rank, local, dist):
                 "wall_ms_per_step": round(te_wall / a.steps * 1e3, 3)},
         "roofline": {"bound": "hbm", "kernel": "k_push + k_segments (one logical push: the takes, the short lists, then the queued long-list segments)",
                      "achieved": round(achieved, 1), "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": None,
-                     "traffic_note": "not measured in this run; an ncu capture of one scale-24 solve of this "
-                                     "command gave 398.7 GB of DRAM traffic for the push kernels against 837 GB "
-                                     "algorithmic (profiles/traffic_all_rmat24.md)",
+                     "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "traffic_note": traffic_note,
                      "alg_bytes_per_solve": int(b_alg), "push_ms_per_solve": round(t_push * 1e3, 3),
                      "pass_ms_per_solve": round(t_all * 1e3, 3),
                      "pass_achieved_gbs": round((b_alg + snap_bytes) / t_all / 1e9, 1) if t_all else None,
@@ -763,6 +797,12 @@ def parse_cli(out):
     f["gpu_wait_s"] = float(mw.group(1)) if mw else None
     mi = re.search(r"cpu io ([0-9.]+)s", out)
     f["cpu_io_s"] = float(mi.group(1)) if mi else None
+    ms = re.search(r"setup ([0-9.]+)s", out)
+    f["setup_s"] = float(ms.group(1)) if ms else None
+    mh = re.search(r"GPU cache load ([0-9.]+)s, pin ([0-9.]+)s, read ([0-9.]+)s", out)
+    if mh:
+        f["host_cache_s"] = {"gpu_cache_load": float(mh.group(1)), "pin": float(mh.group(2)),
+                             "read": float(mh.group(3))}
     return f
 
 

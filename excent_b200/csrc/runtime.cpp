@@ -569,6 +569,7 @@ private:
         host_loop_ = o_.host_cache == "pinned" && !hot_mode_;
         dev_loop_ = (o_.device_loop && cache_mode_ == "chunks" && n_resident_ == nc_ && !hot_mode_) || host_loop_;
         if (!dev_loop_) return 0;
+        const auto t0 = Clock::now();
         for (int c = 0; c < n_resident_; c++) {
             RT_CK(g_.fetch_entries(ch_[c].e0, ch_[c].e1, staging_->entries(0)));
             RT_CK(excent_engine_load_cache(e_, ch_[c].e0, ch_[c].e1, staging_->entries(0)));
@@ -577,10 +578,14 @@ private:
         if (host_loop_) {
             int32_t* h = nullptr;
             ull first = 0;
+            const auto t1 = Clock::now();
             RT_CK(excent_engine_host_cache(e_, &h, &first));
+            const auto t2 = Clock::now();
             if (h) RT_CK(g_.fetch_entries(first, g_.m, h));
-            printf("host cache: pinned, %.2f GB (%d chunks past the GPU cache), lists read in place over the host link\n",
-                   (g_.m - first) * 4.0 / 1e9, nc_ - n_resident_);
+            const auto t3 = Clock::now();
+            printf("host cache: pinned, %.2f GB (%d chunks past the GPU cache), lists read in place over the host link "
+                   "(GPU cache load %.2fs, pin %.2fs, read %.2fs)\n",
+                   (g_.m - first) * 4.0 / 1e9, nc_ - n_resident_, secs(t0, t1), secs(t1, t2), secs(t2, t3));
         }
         return 0;
     }

@@ -476,6 +476,7 @@ def test_sweep_demand_threshold(rmat16, measure, use_graph):
         l0 = eng.launches()
         st = eng.solve(use_graph=use_graph)
         res[(tag, "launches")] = eng.launches() - l0
+        res[(tag, "per_pass")] = res[(tag, "launches")] / (st.passes + 1)
         _, plog = eng.stats(with_log=True)
         res[(tag, "demand")] = [int(p.demand) for p in plog]
         for i, k in enumerate(names):
@@ -490,8 +491,10 @@ def test_sweep_demand_threshold(rmat16, measure, use_graph):
     for k in names:
         for tag in ("some", "none"):
             assert res[(tag, k)]["l1_rel"] <= 1.25 * res[("one", k)]["l1_rel"] + 3e-5, (tag, k, res)
-    assert res[("one", "launches")] <= res[("some", "launches")] + 2 < res[("all", "launches")] + 2
-    assert abs(res[("none", "launches")] - res[("one", "launches")]) <= 2
+    # launches per pass (the orders differ, so do the pass counts): a threshold above every
+    # pass's demand launches like one launch per pass, a threshold inside the range in between
+    assert abs(res[("none", "per_pass")] - res[("one", "per_pass")]) <= 1.0, res
+    assert res[("none", "per_pass")] <= res[("some", "per_pass")] + 0.5 < res[("all", "per_pass")], res
 
 
 @pytest.mark.parametrize("measure", ["pr", "all"])
