@@ -799,10 +799,10 @@ def parse_cli(out):
     f["cpu_io_s"] = float(mi.group(1)) if mi else None
     ms = re.search(r"setup ([0-9.]+)s", out)
     f["setup_s"] = float(ms.group(1)) if ms else None
-    mh = re.search(r"GPU cache load ([0-9.]+)s, pin ([0-9.]+)s, read ([0-9.]+)s", out)
+    mh = re.search(r"GPU cache load ([0-9.]+)s, read ([0-9.]+)s, pinning ([0-9.-]+)s past the read", out)
     if mh:
-        f["host_cache_s"] = {"gpu_cache_load": float(mh.group(1)), "pin": float(mh.group(2)),
-                             "read": float(mh.group(3))}
+        f["host_cache_s"] = {"gpu_cache_load": float(mh.group(1)), "read": float(mh.group(2)),
+                             "pinning_past_the_read": float(mh.group(3))}
     return f
 
 

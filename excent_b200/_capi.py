@@ -122,6 +122,8 @@ PROTOS = [
     ("excent_engine_set_hub_targets", C.c_int, [vp, C.c_int]),
     ("excent_engine_set_hub_order", C.c_int, [vp, C.c_int]),
     ("excent_engine_host_cache", C.c_int, [vp, C.POINTER(vp), u64p]),
+    ("excent_engine_host_cache_begin", C.c_int, [vp, C.POINTER(vp), u64p, C.POINTER(C.c_int)]),
+    ("excent_engine_host_cache_pin", C.c_int, [vp, u64]),
     ("excent_engine_host_pushed", C.c_int, [vp, u64p]),
     ("excent_params_fp64_noalloc", C.c_int, [C.c_int, C.c_int, vp, vp, C.c_double, f64p, vp]),
     ("excent_reference_fp64", C.c_int, [C.c_int, C.c_int, vp, vp, C.c_int, C.c_double, C.c_double, C.c_double,

@@ -125,9 +125,14 @@ int GraphFile::open(const char* path, int io_threads, bool offsets_in_ram, bool 
     if (base == MAP_FAILED) EX_FAIL(EXCENT_ERR_IO, "mmap %s: %s", path, strerror(errno));
     map_.base = base;
     map_.bytes = file_bytes;
-    // lists are touched in demand order: no kernel readahead on faults; the
-    // bulk preads still stream sequentially
-    madvise(base, file_bytes, MADV_RANDOM);
+    // lists are touched in demand order: no kernel readahead on their faults
+    // (the bulk preads still stream sequentially); the offsets are read front
+    // to back (the check below, the upload), so they are read ahead at once
+    const size_t page = (size_t)sysconf(_SC_PAGESIZE);
+    const size_t lists_from = entries_at_ / page * page;
+    madvise(static_cast<char*>(base) + lists_from, file_bytes - lists_from, MADV_RANDOM);
+    madvise(base, lists_from, MADV_SEQUENTIAL);
+    madvise(base, lists_from, MADV_WILLNEED);
     posix_fadvise(fd_, 0, 0, POSIX_FADV_SEQUENTIAL);
     const char* bytes = static_cast<const char*>(base);
     entries_ = reinterpret_cast<const int32_t*>(bytes + entries_at_);

@@ -11,6 +11,9 @@
 //   launch policy                  src/excent.cu:235-240, 629-652
 #include <cuda_runtime.h>
 
+#include <sys/mman.h>
+#include <unistd.h>
+
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -527,11 +530,13 @@ template <int L>
 __global__ void __launch_bounds__(BLOCK) k_segments(void* rv, PushArgs a) {
     typedef typename Lane<L>::T T;
     T* r = reinterpret_cast<T*>(rv);
+    const ull tail = min(a.q->tail, a.hub_cap);
+    // a block none of whose warps has a segment leaves before it zeroes and flushes its slots
+    if ((ull)blockIdx.x * (blockDim.x >> 5) >= tail) return;
     T* hacc = hacc_init<T>(a.hub_k);
     const int lane = threadIdx.x & 31;
     const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    const ull tail = min(a.q->tail, a.hub_cap);
     for (ull i = gw; i < tail; i += nwarps) scatter_segment(a, r, hacc, lane, i);
     hacc_flush(hacc, r, a.hub_id, a.hub_k);
 }
@@ -549,6 +554,16 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
     typedef typename Lane<L>::T T;
     T* x = reinterpret_cast<T*>(a.x);
     T* r = reinterpret_cast<T*>(a.r);
+    const long long first = item_first<SRC>(a), total = item_total<SRC>(a);
+    const long long ntiles = total > first ? (total - first + 31) / 32 : 0;
+    // claims of up to TILE_BATCH tiles, fewer when there are not four claims per warp
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const long long per_claim =
+        a.claim_tiles > 0 ? a.claim_tiles : max(1ll, min((long long)TILE_BATCH, ntiles / (4 * nwarps)));
+    const long long nbatch = (ntiles + per_claim - 1) / per_claim;
+    // with fewer batches than warps, only the first blocks claim: the others leave before they
+    // zero and flush their hub-target slots (a small launch then costs only its active blocks)
+    if ((long long)blockIdx.x * (blockDim.x >> 5) >= nbatch) return;
     T* hacc = hacc_init<T>(a.hub_k);
     // streamed and gathered lists: each tile's short lists arrive in shared memory by one bulk copy
     constexpr bool STAGED = SRC == SRC_CHUNK || SRC == SRC_GATHER;
@@ -565,13 +580,6 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
         if (lane == 0) bar_init(&s_bar[wib]);
         __syncwarp();
     }
-    const long long first = item_first<SRC>(a), total = item_total<SRC>(a);
-    const long long ntiles = total > first ? (total - first + 31) / 32 : 0;
-    // claims of up to TILE_BATCH tiles, fewer when there are not four claims per warp
-    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    const long long per_claim =
-        a.claim_tiles > 0 ? a.claim_tiles : max(1ll, min((long long)TILE_BATCH, ntiles / (4 * nwarps)));
-    const long long nbatch = (ntiles + per_claim - 1) / per_claim;
     ull pushed = 0, hpushed = 0, lanes = 0, taken = 0;
     for (;;) {
     // claim the next batch of tiles (and count this warp as working on it)
@@ -850,6 +858,11 @@ struct excent_engine {
     int hub_k = 0;           // slots in use (0: off)
     int* h_hcache = nullptr; // pinned, mapped host copy of the entries past the device cache
     ull hcache_edges = 0;
+    const int* d_hcache = nullptr;  // its device address, once all of it is pinned
+    // registered in pieces (excent_engine_host_cache_begin/_pin): an anonymous mapping
+    size_t hcache_map_bytes = 0;
+    std::vector<std::pair<char*, size_t>> hcache_pieces;
+    size_t hcache_pinned = 0;       // bytes registered so far, from the start
     int* d_hubv = nullptr;   // high-degree-first order: vertices with lists longer than HUB_MIN
     ull* d_hubv_cnt = nullptr;
     ull hubv_cap = 0;
@@ -904,6 +917,22 @@ static void invalidate_graph(excent_engine* e) {
 }
 
 static void scrub_queues(excent_engine* e);
+// Release the host cache, pinned whole (cudaHostAlloc) or in pieces of an anonymous mapping.
+static void free_host_cache(excent_engine* e) {
+    if (!e->h_hcache) return;
+    if (e->hcache_map_bytes) {
+        for (auto& pc : e->hcache_pieces) cudaHostUnregister(pc.first);
+        munmap(e->h_hcache, e->hcache_map_bytes);
+    } else {
+        cudaFreeHost(e->h_hcache);
+    }
+    e->h_hcache = nullptr;
+    e->d_hcache = nullptr;
+    e->hcache_edges = 0;
+    e->hcache_map_bytes = 0;
+    e->hcache_pieces.clear();
+    e->hcache_pinned = 0;
+}
 static const char* ctrl_error(int err) {
     return err == 3 ? "a push kernel's wait for a bulk copy of its lists timed out"
                     : "device capacity check failed (hub queue overflow)";
@@ -949,7 +978,7 @@ static int free_engine(excent_engine* e) {
         if (s.done) cudaEventDestroy(s.done);
     }
     for (cudaEvent_t ev : e->ev) if (ev) cudaEventDestroy(ev);
-    if (e->h_hcache) cudaFreeHost(e->h_hcache);
+    free_host_cache(e);
     if (e->s_main) cudaStreamDestroy(e->s_main);
     delete e;
     return EXCENT_OK;
@@ -1123,7 +1152,7 @@ extern "C" int excent_engine_reserve_cache(excent_engine* e, unsigned long long 
     EX_CUDA(cudaDeviceSynchronize());
     if (e->d_cache) { cudaFree(e->d_cache); e->d_cache = nullptr; e->cache_edges = 0; }
     e->hub_k = 0;   // a fresh cache holds plain ids
-    if (e->h_hcache) { cudaFreeHost(e->h_hcache); e->h_hcache = nullptr; e->hcache_edges = 0; }
+    free_host_cache(e);
     if (edges == 0) return EXCENT_OK;
     // 4 entries of padding: a bulk copy of a stretch rounds its end up to 16 bytes
     if (cudaMalloc((void**)&e->d_cache, (edges + 4) * sizeof(int)) != cudaSuccess) {
@@ -1286,7 +1315,7 @@ static PushArgs push_args(excent_engine* e, int q) {
     a.hubv = e->d_hubv; a.hubv_cnt = e->d_hubv_cnt; a.skip_hubs = 0; a.chunk = -1; a.stage = 0;
     a.claim_tiles = e->claim_tiles;
     a.hcache = nullptr; a.cache_edges = e->cache_edges;
-    if (e->h_hcache) cudaHostGetDevicePointer((void**)&a.hcache, e->h_hcache, 0);
+    a.hcache = e->d_hcache;
     return a;
 }
 
@@ -1836,12 +1865,12 @@ static int solve_impl(excent_engine* e, double list_frac, int max_passes, int us
     EX_CHECK_ARG(e, "null engine");
     EX_CHECK_ARG(max_passes >= 0 && max_passes < e->log_cap, "max_passes must be < %d", e->log_cap);
     for (int c = 0; c < e->nc; c++)
-        EX_CHECK_ARG(e->loaded[c] || (e->h_hcache && e->ce[c] >= e->cache_edges),
+        EX_CHECK_ARG(e->loaded[c] || (e->d_hcache && e->ce[c] >= e->cache_edges),
                      "chunk %d is neither in the edge cache nor in the host cache", c);
     EX_CUDA(cudaSetDevice(e->dev));
     std::vector<uint8_t> cm(e->nc, 1);
     for (int c = 0; c < e->nc; c++)
-        if (e->h_hcache && e->ce[c] >= e->cache_edges) cm[c] = 2;   // lists in host memory
+        if (e->d_hcache && e->ce[c] >= e->cache_edges) cm[c] = 2;   // lists in host memory
     EX_CUDA(cudaMemcpy(e->d_cmode, cm.data(), e->nc, cudaMemcpyHostToDevice));
     if (init) EX_TRY(init_state(e));
     else EX_TRY(reset_counters(e));
@@ -2188,7 +2217,7 @@ extern "C" int excent_engine_host_cache(excent_engine* e, int32_t** host_edges, 
     EX_CUDA(cudaSetDevice(e->dev));
     invalidate_graph(e);
     EX_CUDA(cudaDeviceSynchronize());
-    if (e->h_hcache) { cudaFreeHost(e->h_hcache); e->h_hcache = nullptr; e->hcache_edges = 0; }
+    free_host_cache(e);
     *host_edges = nullptr;
     const ull cnt = e->m - e->cache_edges;
     if (first_edge) *first_edge = e->cache_edges;
@@ -2199,7 +2228,68 @@ extern "C" int excent_engine_host_cache(excent_engine* e, int32_t** host_edges, 
         EX_FAIL(EXCENT_ERR_NOMEM, "pinned host cache of %llu entries does not fit", cnt);
     }
     e->hcache_edges = cnt;
+    EX_CUDA(cudaHostGetDevicePointer((void**)&e->d_hcache, e->h_hcache, 0));
     *host_edges = e->h_hcache;
+    return EXCENT_OK;
+}
+
+// The host cache in ordinary (pageable) memory, pinned later in pieces: the
+// caller fills it and pins each filled piece (excent_engine_host_cache_pin)
+// while it reads the next, so pinning overlaps the file reads instead of
+// following them (cudaHostAlloc also zero-fills the whole buffer first).
+// pieces_ok = 0: this device cannot address registered memory by its host
+// address, so the whole range must be pinned in one call at the end.
+extern "C" int excent_engine_host_cache_begin(excent_engine* e, int32_t** host_edges, unsigned long long* first_edge,
+                                              int* pieces_ok) {
+    EX_CHECK_ARG(e && host_edges && pieces_ok, "null argument");
+    EX_CUDA(cudaSetDevice(e->dev));
+    invalidate_graph(e);
+    EX_CUDA(cudaDeviceSynchronize());
+    free_host_cache(e);
+    *host_edges = nullptr;
+    const ull cnt = e->m - e->cache_edges;
+    if (first_edge) *first_edge = e->cache_edges;
+    int direct = 0;
+    EX_CUDA(cudaDeviceGetAttribute(&direct, cudaDevAttrCanUseHostPointerForRegisteredMem, e->dev));
+    *pieces_ok = direct;
+    if (cnt == 0) return EXCENT_OK;
+    const size_t page = (size_t)sysconf(_SC_PAGESIZE);
+    const size_t bytes = (cnt * sizeof(int) + page - 1) / page * page;
+    void* p = mmap(nullptr, bytes, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS | MAP_NORESERVE, -1, 0);
+    if (p == MAP_FAILED) EX_FAIL(EXCENT_ERR_NOMEM, "host cache of %llu entries: mmap failed", cnt);
+    e->h_hcache = (int*)p;
+    e->hcache_edges = cnt;
+    e->hcache_map_bytes = bytes;
+    e->hcache_pinned = 0;
+    *host_edges = e->h_hcache;
+    return EXCENT_OK;
+}
+
+// Pin the host cache's entries [0, upto) (relative to its first entry), past
+// what is pinned already; the last call (upto = its size) makes it usable.
+extern "C" int excent_engine_host_cache_pin(excent_engine* e, unsigned long long upto) {
+    EX_CHECK_ARG(e && e->h_hcache && e->hcache_map_bytes, "no host cache begun");
+    EX_CHECK_ARG(upto <= e->hcache_edges, "pin range past the host cache");
+    EX_CUDA(cudaSetDevice(e->dev));
+    const size_t page = (size_t)sysconf(_SC_PAGESIZE);
+    size_t end = upto == e->hcache_edges ? e->hcache_map_bytes : (size_t)upto * sizeof(int) / page * page;
+    if (end <= e->hcache_pinned) return EXCENT_OK;
+    int direct = 0;
+    EX_CUDA(cudaDeviceGetAttribute(&direct, cudaDevAttrCanUseHostPointerForRegisteredMem, e->dev));
+    EX_CHECK_ARG(direct || (e->hcache_pinned == 0 && end == e->hcache_map_bytes),
+                 "this device pins the host cache in one piece only");
+    char* at = (char*)e->h_hcache + e->hcache_pinned;
+    const size_t len = end - e->hcache_pinned;
+    if (cudaHostRegister(at, len, cudaHostRegisterMapped | cudaHostRegisterPortable) != cudaSuccess) {
+        cudaGetLastError();
+        EX_FAIL(EXCENT_ERR_NOMEM, "pinning %zu bytes of the host cache failed", len);
+    }
+    e->hcache_pieces.push_back({at, len});
+    e->hcache_pinned = end;
+    if (end == e->hcache_map_bytes) {
+        if (direct) e->d_hcache = e->h_hcache;
+        else EX_CUDA(cudaHostGetDevicePointer((void**)&e->d_hcache, e->h_hcache, 0));
+    }
     return EXCENT_OK;
 }
 

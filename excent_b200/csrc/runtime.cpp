@@ -14,6 +14,7 @@
 #include <sys/stat.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdlib>
@@ -21,6 +22,7 @@
 #include <memory>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "common.h"
@@ -576,17 +578,56 @@ private:
             loaded_[c] = 1;
         }
         if (host_loop_) {
-            int32_t* h = nullptr;
-            ull first = 0;
             const auto t1 = Clock::now();
-            RT_CK(excent_engine_host_cache(e_, &h, &first));
-            const auto t2 = Clock::now();
-            if (h) RT_CK(g_.fetch_entries(first, g_.m, h));
-            const auto t3 = Clock::now();
+            ull first = 0;
+            double t_read = 0;
+            RT_CK(fill_host_cache(&first, &t_read));
             printf("host cache: pinned, %.2f GB (%d chunks past the GPU cache), lists read in place over the host link "
-                   "(GPU cache load %.2fs, pin %.2fs, read %.2fs)\n",
-                   (g_.m - first) * 4.0 / 1e9, nc_ - n_resident_, secs(t0, t1), secs(t1, t2), secs(t2, t3));
+                   "(GPU cache load %.2fs, read %.2fs, pinning %.2fs past the read)\n",
+                   (g_.m - first) * 4.0 / 1e9, nc_ - n_resident_, secs(t0, t1), t_read,
+                   secs(t1, Clock::now()) - t_read);
         }
+        return 0;
+    }
+
+    // The entries past the GPU cache into host memory, read in 1 GiB pieces by
+    // the reader team; a second thread pins each piece once it is read while
+    // the next one is read (or the whole range after the read, on a device that
+    // cannot address pinned memory by its host address).
+    int fill_host_cache(ull* first, double* t_read) {
+        int32_t* h = nullptr;
+        int pieces_ok = 0;
+        RT_CK(excent_engine_host_cache_begin(e_, &h, first, &pieces_ok));
+        const ull cnt = g_.m - *first;
+        if (!h || cnt == 0) return 0;
+        const ull piece = 1ull << 28;
+        std::atomic<ull> filled{0};
+        std::atomic<int> stop{0};
+        std::string pin_error;
+        std::thread pinner;
+        if (pieces_ok)
+            pinner = std::thread([&] {
+                ull done = 0;
+                while (done < cnt && !stop.load()) {
+                    const ull f = filled.load();
+                    if (f == done) { std::this_thread::sleep_for(std::chrono::milliseconds(2)); continue; }
+                    if (excent_engine_host_cache_pin(e_, f) != EXCENT_OK) { pin_error = excent_last_error(); break; }
+                    done = f;
+                }
+            });
+        const auto r0 = Clock::now();
+        int rc = EXCENT_OK;
+        for (ull at = 0; at < cnt && rc == EXCENT_OK && pin_error.empty(); at += piece) {
+            const ull to = std::min(cnt, at + piece);
+            rc = g_.fetch_entries(*first + at, *first + to, h + at);
+            if (rc == EXCENT_OK) filled.store(to);
+        }
+        *t_read = secs(r0, Clock::now());
+        if (rc != EXCENT_OK) stop.store(1);
+        if (pinner.joinable()) pinner.join();
+        RT_CK(rc);
+        if (!pin_error.empty()) { fprintf(stderr, "excent: %s\n", pin_error.c_str()); return 1; }
+        if (!pieces_ok) RT_CK(excent_engine_host_cache_pin(e_, cnt));
         return 0;
     }
 

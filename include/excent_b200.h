@@ -286,6 +286,16 @@ int excent_engine_autotune(excent_engine* e, double list_frac, int max_passes, e
  * only the lists of pending vertices cross it, with no host-side gather or
  * staging copy. Reserving the edge cache again frees it. */
 int excent_engine_host_cache(excent_engine* e, int32_t** host_edges, unsigned long long* first_edge);
+/* The same host cache, pinned in pieces as the caller fills it: _begin maps
+ * it in pageable memory (nothing pinned, nothing zero-filled ahead of the
+ * reads); _pin(upto) pins its entries [0, upto) past what is pinned already,
+ * so a reader can pin each filled piece while it reads the next. The last
+ * call (upto = m - *first_edge) makes it usable by the solve. *pieces_ok = 0:
+ * the device cannot address registered memory by its host address, so the
+ * whole range must be pinned in that one last call. */
+int excent_engine_host_cache_begin(excent_engine* e, int32_t** host_edges, unsigned long long* first_edge,
+                                   int* pieces_ok);
+int excent_engine_host_cache_pin(excent_engine* e, unsigned long long upto);
 /* Entries pushed from the host cache since the last init (4 bytes each crossed the link). */
 int excent_engine_host_pushed(excent_engine* e, unsigned long long* entries);
 
