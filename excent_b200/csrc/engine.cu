@@ -32,6 +32,7 @@ static constexpr int BLOCK = 256;
 
 enum { SRC_TABLE = 0, SRC_CHUNK = 1, SRC_GATHER = 2, SRC_HOT = 3, SRC_HUBS = 4 };
 enum { WT_NONE = 0, WT_LIST = 1, WT_RANGE = 2 };
+enum { LISTS_ALL = 0, LISTS_SHORT = 1, LISTS_LONG = 2 };
 
 struct HubSeg {
     const int* nb;
@@ -137,7 +138,7 @@ struct PushArgs {
     // (hubv[*hubv_cnt]) first; SRC_TABLE then skips them
     const int* hubv;
     const ull* hubv_cnt;
-    int skip_hubs;      // SRC_TABLE leaves the lists longer than HUB_MIN to SRC_HUBS
+    int lists;          // LISTS_ALL, or only the lists of at most HUB_MIN entries, or only the longer ones
     int chunk;          // SRC_TABLE: only chunk `chunk`'s items (-1: every chunk's)
     int stage;          // SRC_CHUNK / SRC_GATHER: bulk-copy each tile's short lists into shared memory
     int claim_tiles;    // tiles per claim; 0: up to TILE_BATCH, at least four claims per warp
@@ -594,7 +595,7 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
         T p{};
         bool act = false;
         if (get_item<SRC>(a, first + tile * 32 + lane, v, nb, deg) &&
-            !(SRC == SRC_TABLE && a.skip_hubs && deg > HUB_MIN)) {   // pushed by SRC_HUBS
+            !(a.lists == LISTS_SHORT && deg > HUB_MIN) && !(a.lists == LISTS_LONG && deg <= HUB_MIN)) {
             p = take(x, r, v, deg, a.M);
             act = nonzero(p) && deg > 0;
         }
@@ -1312,7 +1313,7 @@ static PushArgs push_args(excent_engine* e, int q) {
     a.hids = e->d_hids; a.hoff = e->d_hoff; a.hedges = e->d_hedges; a.hlist = e->d_hlist;
     a.hubq = e->d_hubq[q]; a.hub_cap = e->hub_cap[q]; a.q = e->d_queue + q; a.ctrl = e->d_ctrl;
     a.hub_id = e->d_hub_id; a.hub_k = e->hub_k;
-    a.hubv = e->d_hubv; a.hubv_cnt = e->d_hubv_cnt; a.skip_hubs = 0; a.chunk = -1; a.stage = 0;
+    a.hubv = e->d_hubv; a.hubv_cnt = e->d_hubv_cnt; a.lists = LISTS_ALL; a.chunk = -1; a.stage = 0;
     a.claim_tiles = e->claim_tiles;
     a.hcache = nullptr; a.cache_edges = e->cache_edges;
     a.hcache = e->d_hcache;
@@ -1332,6 +1333,20 @@ static void launch_push(excent_engine* e, const PushArgs& a, int grid, cudaStrea
         k_segments<4><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a);
     }
     e->launches += 2;
+}
+
+// A streamed or gathered chunk in the pass's high-degree order: with the long
+// lists first (last), one launch takes only those, the next only the others,
+// as the cached push sends its high-degree vertices first (last).
+template <int SRC>
+static void launch_ordered(excent_engine* e, PushArgs a, int grid, cudaStream_t st) {
+    const int order = order_of(e);
+    if (order == 1 || order == 2) {
+        a.lists = order == 1 ? LISTS_LONG : LISTS_SHORT;
+        launch_push<SRC>(e, a, grid, st);
+        a.lists = order == 1 ? LISTS_SHORT : LISTS_LONG;
+    }
+    launch_push<SRC>(e, a, grid, st);
 }
 
 static int grid_for(excent_engine* e, ull items) {
@@ -1376,7 +1391,7 @@ extern "C" int excent_engine_push_cached(excent_engine* e, const unsigned char* 
     PushArgs a = push_args(e, 0);
     a.hot = e->hot_skip ? e->d_hot : nullptr;
     if (order == 1) launch_push<SRC_HUBS>(e, a, e->grid_push, e->s_main);
-    a.skip_hubs = order != 0;
+    a.lists = order != 0 ? LISTS_SHORT : LISTS_ALL;   // the long lists go by SRC_HUBS
     ull demand = 0;
     for (int c = 0; c < e->nc; c++) demand += cnt[2 * c + 1];
     if (sweep_of(e) && demand >= sweep_min_entries(e)) {   // one launch per chunk, in chunk order
@@ -1389,7 +1404,7 @@ extern "C" int excent_engine_push_cached(excent_engine* e, const unsigned char* 
     } else {
         launch_push<SRC_TABLE>(e, a, grid_for(e, total), e->s_main);
     }
-    a.skip_hubs = 0;
+    a.lists = LISTS_ALL;
     if (order == 2) launch_push<SRC_HUBS>(e, a, e->grid_push, e->s_main);
     EX_CUDA(cudaGetLastError());
     return EXCENT_OK;
@@ -1479,7 +1494,7 @@ extern "C" int excent_engine_push_stream(excent_engine* e, int s, int c, const u
     a.stage = e->zc ? 0 : 1;   // mapped host slots are read in place
     if ((double)k < list_frac * nv) { a.ctype = WT_LIST; a.ccount = (unsigned)k; e->n_list++; }
     else { a.ctype = WT_RANGE; a.ccount = (unsigned)nv; e->n_range++; }
-    if (a.ccount) launch_push<SRC_CHUNK>(e, a, grid_for(e, a.ccount), sl.st);
+    if (a.ccount) launch_ordered<SRC_CHUNK>(e, a, grid_for(e, a.ccount), sl.st);
     EX_CUDA(cudaGetLastError());
     if (to_cache) e->loaded[c] = 1;
     EX_CUDA(cudaEventRecord(sl.done, sl.st));
@@ -1501,7 +1516,7 @@ extern "C" int excent_engine_push_gather(excent_engine* e, int s, int k, unsigne
         PushArgs a = push_args(e, 1 + s);
         a.vids = sl.d_vids; a.off = sl.d_off; a.gedges = sl.d_edges; a.gk = (unsigned)k;
         a.stage = e->zc ? 0 : 1;
-        launch_push<SRC_GATHER>(e, a, grid_for(e, (ull)k), sl.st);
+        launch_ordered<SRC_GATHER>(e, a, grid_for(e, (ull)k), sl.st);
         EX_CUDA(cudaGetLastError());
     }
     EX_CUDA(cudaEventRecord(sl.done, sl.st));
@@ -1698,7 +1713,7 @@ static cudaError_t enqueue_push(excent_engine* e, cudaStream_t st, cudaEvent_t* 
         return rc;
     };
     if (order == 1) hub_phase();
-    a.skip_hubs = order != 0;   // the table push skips the high-degree vertices
+    a.lists = order != 0 ? LISTS_SHORT : LISTS_ALL;   // the table push skips the high-degree vertices
     if (use_if) {
         // chunk by chunk: each chunk's push (with its long lists) completes before the next
         // chunk's vertices are taken, so they see everything pushed so far; or the whole table
@@ -1717,7 +1732,7 @@ static cudaError_t enqueue_push(excent_engine* e, cudaStream_t st, cudaEvent_t* 
     } else {
         table(st);
     }
-    a.skip_hubs = 0;
+    a.lists = LISTS_ALL;
     if (ev) cudaEventRecord(ev[3], st);
     if (order == 2) hub_phase();
     if (ev) cudaEventRecord(ev[4], st);

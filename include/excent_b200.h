@@ -237,7 +237,8 @@ int excent_engine_read_trace(excent_engine* e, uint16_t* out);
 int excent_engine_set_hub_targets(excent_engine* e, int k);
 
 /* Order of the high-degree lists (more than 256 entries) in each pass of the
- * device solve and of a host-driven cached push: 1 first, so the large share
+ * device solve, of a host-driven cached push and inside each streamed or
+ * gathered chunk: 1 first, so the large share
  * of a pass's residual they carry reaches the other vertices before those are
  * taken; 2 last, after every other pending vertex; 0 in table order with the
  * rest; -1 (the default) table order when the chunks are swept one by one,
