@@ -221,7 +221,8 @@ class Engine:
         call("excent_engine_autotune", self.h, float(list_frac), int(max_passes), C.byref(best), tried, 16,
              C.byref(nt))
         as_dict = lambda t: {"hub_targets": t.hub_targets, "hub_order": ["table", "first", "last"][t.hub_order],  # noqa: E731
-                             "chunk_sweep": bool(t.chunk_sweep), "ms": round(t.ms, 3)}
+                             "chunk_sweep": bool(t.chunk_sweep), "sweep_demand": t.sweep_demand,
+                             "ms": round(t.ms, 3)}
         return as_dict(best), [as_dict(tried[i]) for i in range(nt.value)]
 
     def scatter_peak(self):

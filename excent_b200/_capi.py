@@ -36,7 +36,8 @@ class PassLog(C.Structure):
 
 
 class Tune(C.Structure):
-    _fields_ = [("hub_targets", C.c_int), ("hub_order", C.c_int), ("chunk_sweep", C.c_int), ("ms", C.c_double)]
+    _fields_ = [("hub_targets", C.c_int), ("hub_order", C.c_int), ("chunk_sweep", C.c_int), ("ms", C.c_double),
+                ("sweep_demand", C.c_double)]
 
 
 class Stats(C.Structure):

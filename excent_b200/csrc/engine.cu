@@ -2165,8 +2165,11 @@ extern "C" int excent_engine_autotune(excent_engine* e, double list_frac, int ma
     auto k = [&](int want) { return std::min(e->n, want); };
     const bool one = e->L == 1;
     const excent_tune cands[] = {
-        {k(2048), 0, 1, 0.0}, {k(one ? 16384 : 4096), 0, 1, 0.0}, {k(512), 0, 1, 0.0},   // table order, swept
-        {k(one ? 16384 : 4096), 1, 0, 0.0}, {k(one ? 4096 : 2048), 1, 0, 0.0}, {0, 1, 0, 0.0},   // lists first
+        // table order, swept while a pass's pending entries reach the demand fraction of m
+        {k(2048), 0, 1, 0.0, 0.5}, {k(2048), 0, 1, 0.0, 0.25}, {k(2048), 0, 1, 0.0, 1.0},
+        {k(one ? 16384 : 4096), 0, 1, 0.0, 0.5}, {k(512), 0, 1, 0.0, 0.5},
+        // the high-degree lists first, one launch per pass
+        {k(one ? 16384 : 4096), 1, 0, 0.0, 0.0}, {k(one ? 4096 : 2048), 1, 0, 0.0, 0.0}, {0, 1, 0, 0.0, 0.0},
     };
     const int nc = (int)(sizeof cands / sizeof cands[0]);
     cudaEvent_t t0, t1;
@@ -2180,6 +2183,7 @@ extern "C" int excent_engine_autotune(excent_engine* e, double list_frac, int ma
         rc = excent_engine_set_hub_targets(e, c.hub_targets);
         if (rc == EXCENT_OK) rc = excent_engine_set_hub_order(e, c.hub_order);
         if (rc == EXCENT_OK) rc = excent_engine_set_chunk_sweep(e, c.chunk_sweep);
+        if (rc == EXCENT_OK && c.chunk_sweep) rc = excent_engine_set_sweep_demand(e, c.sweep_demand);
         if (rc == EXCENT_OK) rc = excent_engine_solve(e, list_frac, max_passes, 1);   // builds the graph
         if (rc != EXCENT_OK) break;
         cudaEventRecord(t0, e->s_main);
@@ -2199,6 +2203,7 @@ extern "C" int excent_engine_autotune(excent_engine* e, double list_frac, int ma
     EX_TRY(excent_engine_set_hub_targets(e, win.hub_targets));
     EX_TRY(excent_engine_set_hub_order(e, win.hub_order));
     EX_TRY(excent_engine_set_chunk_sweep(e, win.chunk_sweep));
+    if (win.chunk_sweep) EX_TRY(excent_engine_set_sweep_demand(e, win.sweep_demand));
     *best = win;
     return EXCENT_OK;
 }

@@ -270,10 +270,12 @@ typedef struct excent_tune {
     int hub_order;     /* 0 table order, 1 high-degree lists first, 2 last */
     int chunk_sweep;   /* 1: one launch per chunk, in chunk order */
     double ms;         /* one solve (graph launch) with these settings */
+    double sweep_demand; /* with chunk_sweep: sweep passes whose pending entries reach this * m */
 } excent_tune;
-/* Time one device solve for each candidate (table order chunk by chunk, or
- * the high-degree lists first in one launch; each with 0 or two sizes of
- * hub-target slots), keep the fastest and return it; tried (cap entries, may
+/* Time one device solve for each candidate and keep the fastest: table order
+ * chunk by chunk (sweep demand 0.25, 0.5 or 1.0 of m; 512, 2048 or the
+ * one-launch count of hub-target slots), or the high-degree lists first in
+ * one launch (0 or two sizes of hub-target slots). tried (cap entries, may
  * be NULL) receives every candidate's time. Needs the whole graph in the edge
  * cache. No counterpart in the reference. */
 int excent_engine_autotune(excent_engine* e, double list_frac, int max_passes, excent_tune* best,

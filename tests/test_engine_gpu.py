@@ -455,6 +455,26 @@ def test_chunk_sweep_matches_one_launch(rmat16, measure, use_graph, order):
 
 
 @pytest.mark.parametrize("measure", ["pr", "all"])
+def test_engine_autotune_keeps_the_fastest_and_solves(rmat16, measure):
+    """excent_engine_autotune times every candidate (swept with three demand thresholds and
+    three slot counts, or high-degree lists first), leaves the engine on the fastest, and the
+    solve with those settings reaches every threshold."""
+    n, idx, adj = rmat16
+    par = O.params(n, idx, adj)
+    kw = dict(alpha=0.9 / par["_lambda"], lam=par["_lambda"], eps_katz=1e-5, eps_ev=1e-5) if measure == "all" else {}
+    meas = X.measures(measure, **kw)
+    eng = make_engine(n, idx, adj, meas, cap=len(adj) // 7 + 1)
+    best, tried = eng.autotune()
+    assert len(tried) == 8
+    assert best["ms"] == min(t["ms"] for t in tried) and all(t["ms"] > 0 for t in tried)
+    assert {t["sweep_demand"] for t in tried if t["chunk_sweep"]} == {0.25, 0.5, 1.0}
+    eng.solve()
+    for i in range(meas.nm):
+        assert np.all(np.abs(eng.read(i, residual=True)) <= np.float32(meas.eps[i]))
+    eng.close()
+
+
+@pytest.mark.parametrize("measure", ["pr", "all"])
 @pytest.mark.parametrize("use_graph", [True, False])
 def test_sweep_demand_threshold(rmat16, measure, use_graph):
     """A sweeping engine with a demand threshold sweeps only the passes whose
