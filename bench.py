@@ -105,8 +105,8 @@ def parse():
     ap.add_argument("--list-frac", type=float, default=0.5,
                     help="per-chunk list/range rule of the device loop (the reference's --list-frac)")
     ap.add_argument("--log-dir", default=None, help="keep the stdout of every CLI run in this directory")
-    ap.add_argument("--hub-order", default="auto", choices=["auto", "first", "last", "table"],
-                    help="where the high-degree lists go in each pass of the device loop (auto: table order when "
+    ap.add_argument("--hub-order", default="auto", choices=["auto", "first", "last", "table", "launch-first"],
+                    help="where the high-degree lists go in each pass of the device loop (auto: launch-first when "
                          "the chunks are swept one by one, else first)")
     ap.add_argument("--chunk-sweep", default="auto", choices=["auto", "on", "off"],
                     help="cached pushes one chunk per launch in chunk order (auto: when there are several chunks)")

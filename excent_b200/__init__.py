@@ -209,7 +209,7 @@ class Engine:
     def set_hub_order(self, order="first"):
         """Device solve: where the lists longer than 256 entries go in each pass
         ("first", "last", or "table": with the rest)."""
-        code = {"auto": -1, "table": 0, "first": 1, "last": 2, False: 0, True: 1}[order]
+        code = {"auto": -1, "table": 0, "first": 1, "last": 2, "launch-first": 3, False: 0, True: 1}[order]
         call("excent_engine_set_hub_order", self.h, code)
 
     def autotune(self, list_frac=0.5, max_passes=100000):
@@ -220,7 +220,8 @@ class Engine:
         nt = C.c_int()
         call("excent_engine_autotune", self.h, float(list_frac), int(max_passes), C.byref(best), tried, 16,
              C.byref(nt))
-        as_dict = lambda t: {"hub_targets": t.hub_targets, "hub_order": ["table", "first", "last"][t.hub_order],  # noqa: E731
+        as_dict = lambda t: {"hub_targets": t.hub_targets,  # noqa: E731
+                             "hub_order": ["table", "first", "last", "launch-first"][t.hub_order],
                              "chunk_sweep": bool(t.chunk_sweep), "sweep_demand": t.sweep_demand,
                              "ms": round(t.ms, 3)}
         return as_dict(best), [as_dict(tried[i]) for i in range(nt.value)]

@@ -941,16 +941,18 @@ static const char* ctrl_error(int err) {
 static int ensure_hubv(excent_engine* e);
 
 // Pass order. By default a graph cut into several chunks is pushed chunk by
-// chunk, each chunk's long lists in their place, which is how the reference
-// launches its resident chunks (src/excent.cu:684-688): every chunk then sees
-// what the earlier ones pushed in the same pass, and a solve pushes about as
-// many entries as the reference's. A single chunk pushes its high-degree
-// lists first instead (measured: fewer entries and smaller errors than table
-// order there). Both can be set explicitly.
+// chunk, which is how the reference launches its resident chunks
+// (src/excent.cu:684-688): every chunk then sees what the earlier ones pushed
+// in the same pass, and a solve pushes about as many entries as the
+// reference's. Inside each launch the chunk's long lists go first (a launch
+// otherwise leaves them to k_segments, after its short lists; first measured
+// smaller errors). A single chunk pushes the graph's high-degree lists first
+// (measured: fewer entries and smaller errors than table order there). Both
+// can be set explicitly.
 static bool sweep_of(const excent_engine* e) { return e->sweep_mode >= 0 ? e->sweep_mode != 0 : e->nc > 1; }
 // A sweeping engine sweeps the passes whose pending entries reach this many.
 static ull sweep_min_entries(const excent_engine* e) { return (ull)(e->sweep_frac * (double)e->m); }
-static int order_of(const excent_engine* e) { return e->hub_order >= 0 ? e->hub_order : (sweep_of(e) ? 0 : 1); }
+static int order_of(const excent_engine* e) { return e->hub_order >= 0 ? e->hub_order : (sweep_of(e) ? 3 : 1); }
 // the order a pass can run: a high-degree order needs the listed high-degree vertices
 static int effective_order(const excent_engine* e);
 
@@ -1325,14 +1327,16 @@ static PushArgs push_args(excent_engine* e, int q) {
 template <int SRC>
 static void launch_push(excent_engine* e, const PushArgs& a, int grid, cudaStream_t st) {
     cudaMemsetAsync(a.q, 0, sizeof(PushQueue), st);
+    // a launch of short lists only queues no segments: no k_segments after it
+    const bool segs = a.lists != LISTS_SHORT;
     if (e->L == 1) {
         k_push<1, SRC><<<grid, BLOCK, hub_smem(e), st>>>(a);
-        k_segments<1><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a);
+        if (segs) k_segments<1><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a);
     } else {
         k_push<4, SRC><<<grid, BLOCK, hub_smem(e), st>>>(a);
-        k_segments<4><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a);
+        if (segs) k_segments<4><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a);
     }
-    e->launches += 2;
+    e->launches += segs ? 2 : 1;
 }
 
 // A streamed or gathered chunk in the pass's high-degree order: with the long
@@ -1341,10 +1345,11 @@ static void launch_push(excent_engine* e, const PushArgs& a, int grid, cudaStrea
 template <int SRC>
 static void launch_ordered(excent_engine* e, PushArgs a, int grid, cudaStream_t st) {
     const int order = order_of(e);
-    if (order == 1 || order == 2) {
-        a.lists = order == 1 ? LISTS_LONG : LISTS_SHORT;
+    if (order != 0) {
+        const bool long_first = order != 2;
+        a.lists = long_first ? LISTS_LONG : LISTS_SHORT;
         launch_push<SRC>(e, a, grid, st);
-        a.lists = order == 1 ? LISTS_SHORT : LISTS_LONG;
+        a.lists = long_first ? LISTS_SHORT : LISTS_LONG;
     }
     launch_push<SRC>(e, a, grid, st);
 }
@@ -1384,14 +1389,24 @@ extern "C" int excent_engine_push_cached(excent_engine* e, const unsigned char* 
     bool all_cached = true;
     for (int c = 0; c < e->nc; c++) all_cached &= cnt[2 * c] == 0 || mode[c] == 1;
     int order = 0;
-    if (all_cached && order_of(e) && !sweep_of(e)) {
+    if (order_of(e) == 3) order = 3;
+    else if (all_cached && order_of(e) && !sweep_of(e)) {
         EX_TRY(ensure_hubv(e));
         order = effective_order(e);
     }
     PushArgs a = push_args(e, 0);
     a.hot = e->hot_skip ? e->d_hot : nullptr;
     if (order == 1) launch_push<SRC_HUBS>(e, a, e->grid_push, e->s_main);
-    a.lists = order != 0 ? LISTS_SHORT : LISTS_ALL;   // the long lists go by SRC_HUBS
+    a.lists = order == 1 || order == 2 ? LISTS_SHORT : LISTS_ALL;   // the long lists go by SRC_HUBS
+    // order 3: each launch's long lists first, then its short ones
+    auto table = [&](unsigned items) {
+        if (order == 3) {
+            a.lists = LISTS_LONG;
+            launch_push<SRC_TABLE>(e, a, grid_for(e, items), e->s_main);
+            a.lists = LISTS_SHORT;
+        }
+        launch_push<SRC_TABLE>(e, a, grid_for(e, items), e->s_main);
+    };
     ull demand = 0;
     for (int c = 0; c < e->nc; c++) demand += cnt[2 * c + 1];
     if (sweep_of(e) && demand >= sweep_min_entries(e)) {   // one launch per chunk, in chunk order
@@ -1399,10 +1414,10 @@ extern "C" int excent_engine_push_cached(excent_engine* e, const unsigned char* 
             const unsigned items = e->h_wt_prefix[c + 1] - e->h_wt_prefix[c];
             if (!items) continue;
             a.chunk = c;
-            launch_push<SRC_TABLE>(e, a, grid_for(e, items), e->s_main);
+            table(items);
         }
     } else {
-        launch_push<SRC_TABLE>(e, a, grid_for(e, total), e->s_main);
+        table(total);
     }
     a.lists = LISTS_ALL;
     if (order == 2) launch_push<SRC_HUBS>(e, a, e->grid_push, e->s_main);
@@ -1645,8 +1660,10 @@ static cudaError_t close_if(cudaStream_t body) {
 // Kernels of one pass outside the per-chunk launches of a chunk sweep, and per
 // chunk launch (for the launch count of a graph solve).
 static void pass_kernels(const excent_engine* e, int order, ull* fixed, ull* per_chunk) {
-    *fixed = 2 + (order == 1 || order == 2 ? 2 : 0) + (sweep_of(e) ? 0 : 2);
-    *per_chunk = sweep_of(e) ? 2 : 0;
+    // kernels of one table push: with segments 2, short lists only 1 (no k_segments)
+    const ull table = order == 3 ? 3 : (order == 1 || order == 2 ? 1 : 2);
+    *fixed = 2 + (order == 1 || order == 2 ? 2 : 0) + (sweep_of(e) ? 0 : table);
+    *per_chunk = sweep_of(e) ? table : 0;
 }
 
 
@@ -1680,16 +1697,18 @@ static cudaError_t enqueue_push(excent_engine* e, cudaStream_t st, cudaEvent_t* 
     // pass's residual reaches every other vertex before that vertex is taken; 2 = last, so they
     // collect the pass's residual and push it once; 0 = in table order with the rest
     const int order = effective_order(e);
+    auto table1 = [&](cudaStream_t s) { launch_push<SRC_TABLE>(e, a, e->grid_push, s); };
+    // order 3: each launch's long lists first, then its short ones
     auto table = [&](cudaStream_t s) {
-        cudaMemsetAsync(a.q, 0, sizeof(PushQueue), s);
-        if (e->L == 1) {
-            k_push<1, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), s>>>(a);
-            k_segments<1><<<e->grid_push, BLOCK, hub_smem(e), s>>>(e->d_r, a);
+        if (order == 3) {
+            a.lists = LISTS_LONG;
+            table1(s);
+            a.lists = LISTS_SHORT;
+            table1(s);
+            a.lists = LISTS_ALL;
         } else {
-            k_push<4, SRC_TABLE><<<e->grid_push, BLOCK, hub_smem(e), s>>>(a);
-            k_segments<4><<<e->grid_push, BLOCK, hub_smem(e), s>>>(e->d_r, a);
+            table1(s);
         }
-        e->launches += 2;
     };
     auto hub_phase = [&]() {
         cudaMemsetAsync(a.q, 0, sizeof(PushQueue), st);
@@ -1713,7 +1732,7 @@ static cudaError_t enqueue_push(excent_engine* e, cudaStream_t st, cudaEvent_t* 
         return rc;
     };
     if (order == 1) hub_phase();
-    a.lists = order != 0 ? LISTS_SHORT : LISTS_ALL;   // the table push skips the high-degree vertices
+    a.lists = order == 1 || order == 2 ? LISTS_SHORT : LISTS_ALL;   // the table push skips the high-degree vertices
     if (use_if) {
         // chunk by chunk: each chunk's push (with its long lists) completes before the next
         // chunk's vertices are taken, so they see everything pushed so far; or the whole table
@@ -1841,6 +1860,7 @@ extern "C" int excent_engine_seed(excent_engine* e, int k, const int32_t* vids, 
 // The vertices whose lists are longer than HUB_MIN (for a high-degree order),
 // listed once per graph; without room for the list the solve runs in table order.
 static int effective_order(const excent_engine* e) {
+    if (order_of(e) == 3) return 3;   // inside each launch: needs no high-degree list
     return order_of(e) && e->d_hubv && !e->hubv_stale ? order_of(e) : 0;
 }
 
@@ -1889,7 +1909,7 @@ static int solve_impl(excent_engine* e, double list_frac, int max_passes, int us
     EX_CUDA(cudaMemcpy(e->d_cmode, cm.data(), e->nc, cudaMemcpyHostToDevice));
     if (init) EX_TRY(init_state(e));
     else EX_TRY(reset_counters(e));
-    if (order_of(e)) EX_TRY(ensure_hubv(e));
+    if (order_of(e) == 1 || order_of(e) == 2) EX_TRY(ensure_hubv(e));
     if (use_graph) {
         EX_TRY(build_graph(e, list_frac, max_passes));
         EX_CUDA(cudaGraphLaunch(e->gexec, e->s_main));
@@ -2076,8 +2096,9 @@ extern "C" int excent_engine_set_hub_targets(excent_engine* e, int k) {
 }
 
 extern "C" int excent_engine_set_hub_order(excent_engine* e, int order) {
-    EX_CHECK_ARG(e && order >= -1 && order <= 2,
-                 "hub order must be 0 (table order), 1 (first), 2 (last) or -1 (by the chunk count)");
+    EX_CHECK_ARG(e && order >= -1 && order <= 3,
+                 "hub order must be 0 (table order), 1 (first), 2 (last), 3 (first in each launch) or -1 (by the "
+                 "chunk count)");
     EX_CUDA(cudaSetDevice(e->dev));
     invalidate_graph(e);
     e->hub_order = order;
@@ -2165,9 +2186,10 @@ extern "C" int excent_engine_autotune(excent_engine* e, double list_frac, int ma
     auto k = [&](int want) { return std::min(e->n, want); };
     const bool one = e->L == 1;
     const excent_tune cands[] = {
-        // table order, swept while a pass's pending entries reach the demand fraction of m
-        {k(2048), 0, 1, 0.0, 0.5}, {k(2048), 0, 1, 0.0, 0.25}, {k(2048), 0, 1, 0.0, 1.0},
-        {k(one ? 16384 : 4096), 0, 1, 0.0, 0.5}, {k(512), 0, 1, 0.0, 0.5},
+        // swept while a pass's pending entries reach the demand fraction of m, each launch's long
+        // lists first (one candidate in plain table order)
+        {k(2048), 3, 1, 0.0, 0.5}, {k(2048), 3, 1, 0.0, 0.25}, {k(2048), 3, 1, 0.0, 1.0},
+        {k(one ? 16384 : 4096), 3, 1, 0.0, 0.5}, {k(2048), 0, 1, 0.0, 0.5},
         // the high-degree lists first, one launch per pass
         {k(one ? 16384 : 4096), 1, 0, 0.0, 0.0}, {k(one ? 4096 : 2048), 1, 0, 0.0, 0.0}, {0, 1, 0, 0.0, 0.0},
     };

@@ -155,8 +155,9 @@ static int parse_options(int argc, char** argv, Options& o) {
                 if (!strcmp(v, "table")) o.hub_order = 0;
                 else if (!strcmp(v, "first")) o.hub_order = 1;
                 else if (!strcmp(v, "last")) o.hub_order = 2;
+                else if (!strcmp(v, "launch-first")) o.hub_order = 3;
                 else if (!strcmp(v, "auto")) o.hub_order = -1;
-                else { fprintf(stderr, "--hub-order must be first, last, table or auto\n"); return 1; }
+                else { fprintf(stderr, "--hub-order must be first, last, launch-first, table or auto\n"); return 1; }
             }
         }
         else { fprintf(stderr, "unknown option %s\n", a.c_str()); return 1; }

@@ -241,8 +241,9 @@ int excent_engine_set_hub_targets(excent_engine* e, int k);
  * gathered chunk: 1 first, so the large share
  * of a pass's residual they carry reaches the other vertices before those are
  * taken; 2 last, after every other pending vertex; 0 in table order with the
- * rest; -1 (the default) table order when the chunks are swept one by one,
- * else first. */
+ * rest; 3 first inside each push launch (each chunk's own long lists before
+ * its other lists, no graph-wide list); -1 (the default) 3 when the chunks are
+ * swept one by one, else 1. */
 int excent_engine_set_hub_order(excent_engine* e, int order);
 /* Cached pushes chunk by chunk (1: one launch per chunk, each after the
  * previous one, as the reference launches its resident chunks on one stream,
@@ -272,10 +273,10 @@ typedef struct excent_tune {
     double ms;         /* one solve (graph launch) with these settings */
     double sweep_demand; /* with chunk_sweep: sweep passes whose pending entries reach this * m */
 } excent_tune;
-/* Time one device solve for each candidate and keep the fastest: table order
- * chunk by chunk (sweep demand 0.25, 0.5 or 1.0 of m; 512, 2048 or the
- * one-launch count of hub-target slots), or the high-degree lists first in
- * one launch (0 or two sizes of hub-target slots). tried (cap entries, may
+/* Time one device solve for each candidate and keep the fastest: chunk by
+ * chunk, each launch's long lists first (sweep demand 0.25, 0.5 or 1.0 of m;
+ * 2048 or the one-launch count of hub-target slots) or in table order, or the
+ * graph's high-degree lists first in one launch (0 or two sizes of slots). tried (cap entries, may
  * be NULL) receives every candidate's time. Needs the whole graph in the edge
  * cache. No counterpart in the reference. */
 int excent_engine_autotune(excent_engine* e, double list_frac, int max_passes, excent_tune* best,
