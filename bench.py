@@ -52,7 +52,7 @@ T_START = time.perf_counter()
 # DRAM bytes (read + write) of the push kernels per solve, GB, from the ncu captures summarised in
 # profiles/ (dram__bytes_read.sum + dram__bytes_write.sum, one pass per launch, three solves)
 TRAFFIC_CAPTURES = {
-    ("cached-all", 24): (302.4, "GB per solve: k_push 113.7 + k_segments 188.7, ncu over three solves of "
+    ("cached-all", 24): (307.0, "GB per solve: k_push 118.3 + k_segments 188.7, ncu over three solves of "
                                 "`bench.py --steps 1 --warmup 0 --no-cpu-baseline --errors off --no-graph` "
                                 "(profiles/traffic_all_rmat24.md); `achieved` and `traffic` are both per solve"),
 }
