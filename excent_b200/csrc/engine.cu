@@ -1810,12 +1810,11 @@ static int build_graph(excent_engine* e, double list_frac, int max_passes) {
     return EXCENT_OK;
 }
 
-// After a device-side failure, a segment may have been left marked written:
-// clear every queue (and the flag) so no later launch reads one.
+// After a device-side failure (a segment queue overflow, a bulk-copy wait that
+// gave up): wait for the device, then clear the queue counters and the flag so
+// the next solve starts clean.
 static void scrub_queues(excent_engine* e) {
     cudaDeviceSynchronize();
-    for (int q = 0; q < 3; q++)
-        if (e->d_hubq[q]) cudaMemset(e->d_hubq[q], 0, e->hub_cap[q] * sizeof(HubSeg));
     cudaMemset(e->d_queue, 0, 3 * sizeof(PushQueue));
     cudaMemset(&e->d_ctrl->err, 0, sizeof(int));
     cudaDeviceSynchronize();
