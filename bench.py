@@ -298,7 +298,7 @@ def error_report(a, n, m, d_idx, d_adj, idx_np, adj_np, v0, e, eng, meas, measur
             args += ["--alpha", "%.9g" % alpha, "--beta", "1", "--lambda", "%.17g" % lam, "--eps-katz", "1e-6",
                      "--eps-ev", "1e-6"]
         import re
-        runs, passes = [], []
+        runs, passes, pushed_x_m = [], [], []
         for _ in range(a.error_runs):
             r = subprocess.run([ref_bin, *args], capture_output=True, text=True, timeout=1800,
                                env=dict(os.environ, HOME=d))
@@ -307,10 +307,12 @@ def error_report(a, n, m, d_idx, d_adj, idx_np, adj_np, v0, e, eng, meas, measur
                 return rep
             mp = re.search(r"^passes (\d+)", r.stdout, re.M)
             passes.append(int(mp.group(1)) if mp else None)
+            mx = re.search(r"edges pushed: ([0-9.]+) x", r.stdout)
+            pushed_x_m.append(float(mx.group(1)) if mx else None)
             runs.append({k: error_vs_fp64(k, ref[k], np.fromfile(os.path.join(d, f"out.{k}.bin"), dtype=np.float32))
                          for k in kinds})
         rep["reference_engine"] = {"args": " ".join(args[1:]).replace(d, "<tmp>"), "passes": passes,
-                                   **median_errors(runs)}
+                                   "pushed_x_m": pushed_x_m, **median_errors(runs)}
     finally:
         shutil.rmtree(d, ignore_errors=True)
     return rep
@@ -944,6 +946,11 @@ def run_ooc(a, world, rank, local, dist):
         del ballast
         head = "ours_pinned" if a.ooc_mode == "pinned" else "ours"
         ours = runs.get(f"{a.ooc_measures.split(',')[0]}/{head}", {})
+        refr = runs.get(f"{a.ooc_measures.split(',')[0]}/reference", {})
+        if "passes_s" in ours and "link_bytes" in refr:
+            # the link bound counted on the reference's own bytes shipped (src/excent.cu:699, :730)
+            ours["link_bound_on_reference_bytes_s"] = round(refr["link_bytes"] / (link * 1e9), 3)
+            ours["frac_of_reference_bytes_bound"] = round(refr["link_bytes"] / (link * 1e9) / ours["passes_s"], 4)
         if "passes_s" not in ours:
             return {"metric": "GTEPS (out of core)", "unavailable": f"CLI run failed: {ours}"}
         return {
