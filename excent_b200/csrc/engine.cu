@@ -142,7 +142,6 @@ struct PushArgs {
     int chunk;          // SRC_TABLE: only chunk `chunk`'s items (-1: every chunk's)
     int stage;          // SRC_CHUNK / SRC_GATHER: bulk-copy each tile's short lists into shared memory
     int claim_tiles;    // tiles per claim; 0: up to TILE_BATCH, at least four claims per warp
-    int drain;          // first scatter the segments the previous launch on the stream queued in q
     // lists past the device cache read in place from pinned host memory (zero copy)
     const int* hcache;   // entries [cache_edges, m), device-mapped
     ull cache_edges;
@@ -563,11 +562,9 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
     const long long per_claim =
         a.claim_tiles > 0 ? a.claim_tiles : max(1ll, min((long long)TILE_BATCH, ntiles / (4 * nwarps)));
     const long long nbatch = (ntiles + per_claim - 1) / per_claim;
-    // segments queued by the previous launch, scattered before this launch's own tiles
-    const long long drain = a.drain ? (long long)min(a.q->tail, a.hub_cap) : 0;
-    // with fewer batches (and segments) than warps, only the first blocks work: the others leave
-    // before they zero and flush their hub-target slots (a small launch costs only its active blocks)
-    if ((long long)blockIdx.x * (blockDim.x >> 5) >= max(nbatch, drain)) return;
+    // with fewer batches than warps, only the first blocks claim: the others leave before they
+    // zero and flush their hub-target slots (a small launch then costs only its active blocks)
+    if ((long long)blockIdx.x * (blockDim.x >> 5) >= nbatch) return;
     T* hacc = hacc_init<T>(a.hub_k);
     // streamed and gathered lists: each tile's short lists arrive in shared memory by one bulk copy
     constexpr bool STAGED = SRC == SRC_CHUNK || SRC == SRC_GATHER;
@@ -583,10 +580,6 @@ __global__ void __launch_bounds__(BLOCK) k_push(PushArgs a) {
     if (stage_on) {
         if (lane == 0) bar_init(&s_bar[wib]);
         __syncwarp();
-    }
-    if (drain) {
-        const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-        for (long long i = gw; i < drain; i += nwarps) scatter_segment(a, r, hacc, lane, (ull)i);
     }
     ull pushed = 0, hpushed = 0, lanes = 0, taken = 0;
     for (;;) {
@@ -1322,7 +1315,7 @@ static PushArgs push_args(excent_engine* e, int q) {
     a.hids = e->d_hids; a.hoff = e->d_hoff; a.hedges = e->d_hedges; a.hlist = e->d_hlist;
     a.hubq = e->d_hubq[q]; a.hub_cap = e->hub_cap[q]; a.q = e->d_queue + q; a.ctrl = e->d_ctrl;
     a.hub_id = e->d_hub_id; a.hub_k = e->hub_k;
-    a.hubv = e->d_hubv; a.hubv_cnt = e->d_hubv_cnt; a.lists = LISTS_ALL; a.chunk = -1; a.stage = 0; a.drain = 0;
+    a.hubv = e->d_hubv; a.hubv_cnt = e->d_hubv_cnt; a.lists = LISTS_ALL; a.chunk = -1; a.stage = 0;
     a.claim_tiles = e->claim_tiles;
     a.hcache = nullptr; a.cache_edges = e->cache_edges;
     a.hcache = e->d_hcache;
@@ -1332,18 +1325,10 @@ static PushArgs push_args(excent_engine* e, int q) {
 // One push launch: its work queue zeroed, then the kernel (which scatters its
 // own long-list segments).
 template <int SRC>
-static void launch_push(excent_engine* e, const PushArgs& a, int grid, cudaStream_t st, bool segs_after = true) {
-    // a draining launch keeps the queued segments and resets only the tile claims; it runs on
-    // the whole grid, whose warps share out the segments
-    if (a.drain) {
-        cudaMemsetAsync(&a.q->claim, 0, sizeof(ull), st);
-        grid = e->grid_push;
-    } else {
-        cudaMemsetAsync(a.q, 0, sizeof(PushQueue), st);
-    }
-    // k_segments after the launch, unless the next launch drains its segments or it queues
-    // none (short lists only)
-    const bool segs = segs_after && a.lists != LISTS_SHORT;
+static void launch_push(excent_engine* e, const PushArgs& a, int grid, cudaStream_t st) {
+    cudaMemsetAsync(a.q, 0, sizeof(PushQueue), st);
+    // a launch of short lists only queues no segments: no k_segments after it
+    const bool segs = a.lists != LISTS_SHORT;
     if (e->L == 1) {
         k_push<1, SRC><<<grid, BLOCK, hub_smem(e), st>>>(a);
         if (segs) k_segments<1><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a);
@@ -1360,15 +1345,11 @@ static void launch_push(excent_engine* e, const PushArgs& a, int grid, cudaStrea
 template <int SRC>
 static void launch_ordered(excent_engine* e, PushArgs a, int grid, cudaStream_t st) {
     const int order = order_of(e);
-    if (order == 2) {
-        a.lists = LISTS_SHORT;
+    if (order != 0) {
+        const bool long_first = order != 2;
+        a.lists = long_first ? LISTS_LONG : LISTS_SHORT;
         launch_push<SRC>(e, a, grid, st);
-        a.lists = LISTS_LONG;
-    } else if (order != 0) {   // long lists first; the short-list launch drains their segments
-        a.lists = LISTS_LONG;
-        launch_push<SRC>(e, a, grid, st, false);
-        a.lists = LISTS_SHORT;
-        a.drain = 1;
+        a.lists = long_first ? LISTS_SHORT : LISTS_LONG;
     }
     launch_push<SRC>(e, a, grid, st);
 }
@@ -1415,28 +1396,20 @@ extern "C" int excent_engine_push_cached(excent_engine* e, const unsigned char* 
     }
     PushArgs a = push_args(e, 0);
     a.hot = e->hot_skip ? e->d_hot : nullptr;
-    ull demand = 0;
-    for (int c = 0; c < e->nc; c++) demand += cnt[2 * c + 1];
-    const bool swept = sweep_of(e) && demand >= sweep_min_entries(e);
-    // with the high-degree lists first and one table launch, that launch drains their segments
-    const bool fuse_hubs = order == 1 && !swept;
-    if (order == 1) launch_push<SRC_HUBS>(e, a, e->grid_push, e->s_main, !fuse_hubs);
+    if (order == 1) launch_push<SRC_HUBS>(e, a, e->grid_push, e->s_main);
     a.lists = order == 1 || order == 2 ? LISTS_SHORT : LISTS_ALL;   // the long lists go by SRC_HUBS
-    a.drain = fuse_hubs ? 1 : 0;
-    // order 3: each launch's long lists first, then its short ones, which drain their segments
+    // order 3: each launch's long lists first, then its short ones
     auto table = [&](unsigned items) {
         if (order == 3) {
             a.lists = LISTS_LONG;
-            launch_push<SRC_TABLE>(e, a, grid_for(e, items), e->s_main, false);
+            launch_push<SRC_TABLE>(e, a, grid_for(e, items), e->s_main);
             a.lists = LISTS_SHORT;
-            a.drain = 1;
-            launch_push<SRC_TABLE>(e, a, grid_for(e, items), e->s_main);
-            a.drain = 0;
-        } else {
-            launch_push<SRC_TABLE>(e, a, grid_for(e, items), e->s_main);
         }
+        launch_push<SRC_TABLE>(e, a, grid_for(e, items), e->s_main);
     };
-    if (swept) {   // one launch per chunk, in chunk order
+    ull demand = 0;
+    for (int c = 0; c < e->nc; c++) demand += cnt[2 * c + 1];
+    if (sweep_of(e) && demand >= sweep_min_entries(e)) {   // one launch per chunk, in chunk order
         for (int c = 0; c < e->nc; c++) {
             const unsigned items = e->h_wt_prefix[c + 1] - e->h_wt_prefix[c];
             if (!items) continue;
@@ -1447,7 +1420,6 @@ extern "C" int excent_engine_push_cached(excent_engine* e, const unsigned char* 
         table(total);
     }
     a.lists = LISTS_ALL;
-    a.drain = 0;
     if (order == 2) launch_push<SRC_HUBS>(e, a, e->grid_push, e->s_main);
     EX_CUDA(cudaGetLastError());
     return EXCENT_OK;
@@ -1688,14 +1660,10 @@ static cudaError_t close_if(cudaStream_t body) {
 // Kernels of one pass outside the per-chunk launches of a chunk sweep, and per
 // chunk launch (for the launch count of a graph solve).
 static void pass_kernels(const excent_engine* e, int order, ull* fixed, ull* per_chunk) {
-    const bool sweep = sweep_of(e);
-    // kernels of one table push: a launch and its k_segments (2); short lists only, no segments
-    // of their own (1); each launch's long lists, then the short ones draining them (2)
-    const ull table = order == 1 || order == 2 ? 1 : 2;
-    // the high-degree launch, and its k_segments unless the one table launch drains them
-    const ull hubs = order == 1 ? (sweep ? 2 : 1) : (order == 2 ? 2 : 0);
-    *fixed = 2 + hubs + (sweep ? 0 : table);
-    *per_chunk = sweep ? table : 0;
+    // kernels of one table push: with segments 2, short lists only 1 (no k_segments)
+    const ull table = order == 3 ? 3 : (order == 1 || order == 2 ? 1 : 2);
+    *fixed = 2 + (order == 1 || order == 2 ? 2 : 0) + (sweep_of(e) ? 0 : table);
+    *per_chunk = sweep_of(e) ? table : 0;
 }
 
 
@@ -1729,28 +1697,29 @@ static cudaError_t enqueue_push(excent_engine* e, cudaStream_t st, cudaEvent_t* 
     // pass's residual reaches every other vertex before that vertex is taken; 2 = last, so they
     // collect the pass's residual and push it once; 0 = in table order with the rest
     const int order = effective_order(e);
-    // with the high-degree lists first and one table launch per pass, that launch drains
-    // their segments (with a sweep a chunk's launch may be skipped, so k_segments does)
-    const bool fuse_hubs = order == 1 && !sweep_of(e);
-    // order 3: each launch's long lists first, then its short ones, which drain their segments
+    auto table1 = [&](cudaStream_t s) { launch_push<SRC_TABLE>(e, a, e->grid_push, s); };
+    // order 3: each launch's long lists first, then its short ones
     auto table = [&](cudaStream_t s) {
         if (order == 3) {
             a.lists = LISTS_LONG;
-            launch_push<SRC_TABLE>(e, a, e->grid_push, s, false);
+            table1(s);
             a.lists = LISTS_SHORT;
-            a.drain = 1;
-            launch_push<SRC_TABLE>(e, a, e->grid_push, s);
+            table1(s);
             a.lists = LISTS_ALL;
-            a.drain = 0;
         } else {
-            launch_push<SRC_TABLE>(e, a, e->grid_push, s);
+            table1(s);
         }
     };
-    auto hub_phase = [&](bool segs) {
-        const int keep = a.lists;
-        a.lists = LISTS_ALL;
-        launch_push<SRC_HUBS>(e, a, e->grid_push, st, segs);
-        a.lists = keep;
+    auto hub_phase = [&]() {
+        cudaMemsetAsync(a.q, 0, sizeof(PushQueue), st);
+        if (e->L == 1) {
+            k_push<1, SRC_HUBS><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
+            k_segments<1><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a);
+        } else {
+            k_push<4, SRC_HUBS><<<e->grid_push, BLOCK, hub_smem(e), st>>>(a);
+            k_segments<4><<<e->grid_push, BLOCK, hub_smem(e), st>>>(e->d_r, a);
+        }
+        e->launches += 2;
     };
     // one launch under an IF node (c = -1: the whole table)
     auto guarded = [&](int c) -> cudaError_t {
@@ -1762,9 +1731,8 @@ static cudaError_t enqueue_push(excent_engine* e, cudaStream_t st, cudaEvent_t* 
         a.chunk = -1;
         return rc;
     };
-    if (order == 1) hub_phase(!fuse_hubs);
+    if (order == 1) hub_phase();
     a.lists = order == 1 || order == 2 ? LISTS_SHORT : LISTS_ALL;   // the table push skips the high-degree vertices
-    a.drain = fuse_hubs ? 1 : 0;
     if (use_if) {
         // chunk by chunk: each chunk's push (with its long lists) completes before the next
         // chunk's vertices are taken, so they see everything pushed so far; or the whole table
@@ -1784,9 +1752,8 @@ static cudaError_t enqueue_push(excent_engine* e, cudaStream_t st, cudaEvent_t* 
         table(st);
     }
     a.lists = LISTS_ALL;
-    a.drain = 0;
     if (ev) cudaEventRecord(ev[3], st);
-    if (order == 2) hub_phase(true);
+    if (order == 2) hub_phase();
     if (ev) cudaEventRecord(ev[4], st);
     return cudaGetLastError();
 }
