@@ -293,7 +293,7 @@ def error_report(a, n, m, d_idx, d_adj, idx_np, adj_np, v0, e, eng, meas, measur
         path = os.path.join(d, "g.egr")
         X.write_egr(path, idx_np, adj_np)
         args = [path, "--measure", measure, "--cache", "chunks", "--stream-ratio", "2", "--dump",
-                os.path.join(d, "out"), "--max-passes", str(a.ref_passes)]
+                os.path.join(d, "out"), "--max-passes", str(a.ref_passes), "--count-pushes"]
         if measure == "all":
             args += ["--alpha", "%.9g" % alpha, "--beta", "1", "--lambda", "%.17g" % lam, "--eps-katz", "1e-6",
                      "--eps-ev", "1e-6"]
