@@ -71,3 +71,20 @@ def test_engine_create_fails_with_status_without_gpu():
     with pytest.raises(X.ExcentError) as ei:
         X.Engine(10, 0, M, [0], [0, 0])
     assert ei.value.code == 2
+
+
+@pytest.mark.parametrize("name,args", [
+    ("excent_engine_set_sweep_demand", [None, 0.5]),
+    ("excent_engine_set_claim_tiles", [None, 4]),
+    ("excent_engine_set_chunk_sweep", [None, -1]),
+    ("excent_engine_set_hub_order", [None, 3]),
+    ("excent_engine_host_cache_pin", [None, 0]),
+    ("excent_engine_host_cache_begin", [None, None, None, None]),
+    ("excent_engine_autotune", [None, 0.5, 100, None, None, 0, None]),
+])
+def test_engine_entries_reject_a_null_engine(name, args):
+    """The pass-order, tuning and host-cache entries check their arguments before any CUDA call."""
+    import excent_b200._capi as K
+    L = K.load()
+    assert getattr(L, name)(*args) == 1
+    assert L.excent_last_error()
